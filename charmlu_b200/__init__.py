@@ -1,0 +1,216 @@
+"""charmlu_b200 — B200-native dense LU with partial pivoting + solve.
+
+Host-side mirror of charmlu's driver interface for its factor-then-solve
+path.  charmlu configures a run with ``LUConfig`` (luConfig.h:8-62: matrix
+size, block size, pivot batch size, memory threshold), starts it with
+``LUSolver`` (benchmark.C:222-401: factor, then forwardSolve on the
+diagonals, then validation through the scaled residual).  Here the same
+objects drive the C ABI of ``liblu_b200.so`` on one GPU; device memory and
+streams come from PyTorch (plumbing only).  There is no CPU fallback: a
+missing library or a CPU tensor raises.
+"""
+import ctypes
+import dataclasses
+
+import torch
+
+from . import _lib
+from ._lib import (LU_ERR_ARG, LU_ERR_NOCONV, LU_ERR_TIMEOUT, LU_ERR_UNSUPPORTED, LU_IR_CLASSIC, LU_IR_GMRES, LU_OK,
+                   LU_PREC_BF16, LU_PREC_FP16S, LU_PREC_FP64)
+
+__all__ = ["LUConfig", "LUSolver", "LUError", "generate_uniform", "matgen", "status_string",
+           "LU_PREC_FP64", "LU_PREC_BF16", "LU_PREC_FP16S", "LU_IR_CLASSIC", "LU_IR_GMRES"]
+
+EPS = 2.220446049250313e-16
+
+
+class LUError(RuntimeError):
+    def __init__(self, code, what=""):
+        self.code = code
+        super().__init__(f"{what}: {status_string(code)} ({code})")
+
+
+def status_string(code):
+    return _lib.load().lu_status_string(int(code)).decode()
+
+
+def _check(code, what):
+    if code != LU_OK:
+        raise LUError(code, what)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _require_cuda(t, dtype, name):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor (no CPU path exists)")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+
+
+@dataclasses.dataclass
+class LUConfig:
+    """luConfig.h:8-62 (matrixSize, blockSize, pivotBatchSize, memThreshold)
+    plus the B200 additions.  memThreshold and the mapping fields exist for
+    CLI compatibility and have no effect on one GPU."""
+    matrix_size: int
+    block_size: int = 128
+    pivot_batch_size: int = 0          # 0 -> blockSize/4 (benchmark.C:98)
+    mem_threshold: int = 0             # MB; ignored (one GPU holds the matrix)
+    precision: int = LU_PREC_FP64
+    lookahead: bool = False
+    use_graph: bool = False
+    ir_mode: int = LU_IR_CLASSIC
+    ir_max_iter: int = 50
+    ir_target: float = 16.0
+    sing_threshold: float = 0.0        # reference: 100*eps aborts (lu.ci:339)
+    spin_limit: int = 0
+
+    def to_c(self):
+        c = _lib.LuConfig()
+        _check(_lib.load().lu_config_default(ctypes.byref(c), int(self.matrix_size), int(self.block_size)),
+               "lu_config_default")
+        if self.pivot_batch_size:
+            c.pivot_batch = int(self.pivot_batch_size)
+        c.precision = int(self.precision)
+        c.lookahead = int(bool(self.lookahead))
+        c.use_graph = int(bool(self.use_graph))
+        c.ir_mode = int(self.ir_mode)
+        c.ir_max_iter = int(self.ir_max_iter)
+        c.ir_target = float(self.ir_target)
+        c.sing_threshold = float(self.sing_threshold)
+        c.spin_limit = int(self.spin_limit)
+        return c
+
+
+class LUSolver:
+    """One solver handle on the current CUDA device (LUSolver, benchmark.C:222-401)."""
+
+    def __init__(self, cfg: LUConfig):
+        if cfg.matrix_size <= 0 or cfg.block_size <= 0:
+            raise LUError(LU_ERR_ARG, "LUConfig")
+        self.cfg = cfg
+        self._L = _lib.load()
+        self._c = cfg.to_c()
+        h = ctypes.c_void_p()
+        _check(self._L.lu_create(ctypes.byref(self._c), ctypes.byref(h)), "lu_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.lu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def n(self):
+        return self.cfg.matrix_size
+
+    def workspace_bytes(self):
+        return int(self._L.lu_workspace_bytes(ctypes.byref(self._c)))
+
+    # -- status --------------------------------------------------------
+    def status(self, stream=None):
+        """Synchronise and return LU_OK, >0 (singular column) or LU_ERR_*."""
+        return int(self._L.lu_status(self._h, _stream(stream)))
+
+    def check(self, what="lu", stream=None):
+        st = self.status(stream)
+        if st != LU_OK:
+            raise LUError(st, what)
+
+    # -- factor / solve ------------------------------------------------
+    def _check_matrix(self, A):
+        _require_cuda(A, torch.float64, "A")
+        n = self.n
+        if A.dim() != 2 or A.shape[0] != n or A.shape[1] != n or A.stride(1) != 1:
+            raise LUError(LU_ERR_ARG, "A must be n x n with unit column stride")
+        return A.stride(0)
+
+    def factor(self, A, ipiv=None, rhs=None, stream=None):
+        """In-place P A = L U (LUBlk::factor, lu.ci:31-42).  Returns ipiv
+        (int32, 0-based global rows).  rhs, if given, is permuted with the
+        rows (lu.h:66)."""
+        lda = self._check_matrix(A)
+        if ipiv is None:
+            ipiv = torch.empty(self.n, dtype=torch.int32, device=A.device)
+        if rhs is not None:
+            _require_cuda(rhs, torch.float64, "rhs")
+        _check(self._L.lu_factor(self._h, _ptr(A), lda, _ptr(ipiv), _ptr(rhs), _stream(stream)), "lu_factor")
+        return ipiv
+
+    def solve(self, LU, ipiv, B, trans=False, stream=None):
+        """Solve with stored factors in place (forwardSolve/backwardSolve,
+        lu.ci:387-436); trans=True solves A^T X = B."""
+        lda = self._check_matrix(LU)
+        _require_cuda(B, torch.float64, "B")
+        Bv = B if B.dim() == 2 else B.view(-1, 1)
+        if Bv.stride(1) != 1 and Bv.shape[1] > 1:
+            raise LUError(LU_ERR_ARG, "B must be row-major")
+        ldb = Bv.stride(0) if Bv.shape[1] > 1 else 1
+        _check(self._L.lu_solve(self._h, _ptr(LU), lda, _ptr(ipiv), _ptr(Bv), ldb, Bv.shape[1], int(trans),
+                                _stream(stream)), "lu_solve")
+        return B
+
+    def factor_solve(self, A, b, ipiv=None, stream=None):
+        """Time-to-solution span of the reference (benchmark.C:243 -> 344):
+        factor A in place and overwrite b with x."""
+        lda = self._check_matrix(A)
+        _require_cuda(b, torch.float64, "b")
+        if ipiv is None:
+            ipiv = torch.empty(self.n, dtype=torch.int32, device=A.device)
+        _check(self._L.lu_factor_solve(self._h, _ptr(A), lda, _ptr(ipiv), _ptr(b), _stream(stream)),
+               "lu_factor_solve")
+        return ipiv
+
+    def residual(self, A, x, b, stream=None):
+        """Scaled residual against the ORIGINAL A (benchmark.C:385-400).
+        Returns dict(amax, anorm, bnorm, xnorm, rnorm, r_ref, r_hpl)."""
+        lda = self._check_matrix(A)
+        info = _lib.LuResidualInfo()
+        _check(self._L.lu_residual(self._h, _ptr(A), lda, _ptr(x), _ptr(b), ctypes.byref(info), _stream(stream)),
+               "lu_residual")
+        return {k: getattr(info, k) for k, _ in info._fields_}
+
+    def refine_solve(self, A, b, x=None, stream=None):
+        """Mixed-precision factor + FP64 iterative refinement (A, b untouched)."""
+        lda = self._check_matrix(A)
+        _require_cuda(b, torch.float64, "b")
+        if x is None:
+            x = torch.empty_like(b)
+        info = _lib.LuRefineInfo()
+        _check(self._L.lu_refine_solve(self._h, _ptr(A), lda, _ptr(b), _ptr(x), ctypes.byref(info),
+                                       _stream(stream)), "lu_refine_solve")
+        return x, {k: getattr(info, k) for k, _ in info._fields_}
+
+
+def generate_uniform(rows, cols, seed=42, stream_id=0, device="cuda", out=None):
+    """Counter-based uniform[-0.5,0.5) matrix, identical to the oracle's."""
+    if out is None:
+        out = torch.empty(rows, cols, dtype=torch.float64, device=device)
+    _require_cuda(out, torch.float64, "out")
+    ld = out.stride(0) if out.dim() == 2 else cols
+    _check(_lib.load().lu_generate_uniform(_ptr(out), int(rows), int(cols), int(ld), int(seed), int(stream_id),
+                                           _stream()), "lu_generate_uniform")
+    return out
+
+
+def matgen(count, seed=9934835, skip=0):
+    """The reference's b generator MatGen (benchmark.C:28-74), host side."""
+    import numpy as np
+    out = np.empty(int(count), dtype=np.float64)
+    _check(_lib.load().lu_matgen_host(ctypes.c_void_p(out.ctypes.data), int(count), int(seed), int(skip)),
+           "lu_matgen_host")
+    return out

@@ -1,0 +1,82 @@
+// Internal launcher declarations shared by the host orchestration.
+#pragma once
+#include "common.cuh"
+
+namespace lub {
+
+// ---- C -= A * B (row-major sub-blocks addressed through tensor maps)
+struct GemmArgs {
+  int a_row0, a_col0;  // origin of A in mapA's matrix
+  int b_row0, b_col0;  // origin of B in mapB's matrix
+  double* C;           // origin of C
+  int64_t ldc;
+  int M, N, K;
+  DevStatus* st;
+  long long spin;
+};
+int gemm_f64_init();
+int gemm_f64_smem_bytes();
+int launch_gemm_f64_sub(const CUtensorMap& mapA, const CUtensorMap& mapB, const GemmArgs& a, cudaStream_t s);
+
+// FP32 SIMT GEMM C -= A * B (panel / TRSM halves of the mixed path)
+int launch_gemm_f32_sub(const float* A, int64_t lda, const float* B, int64_t ldb, float* C, int64_t ldc, int M,
+                        int N, int K, cudaStream_t s);
+
+// ---- unblocked panel leaf (cooperative, rows resident in shared memory)
+template <typename T>
+struct LeafScratch {
+  T* cand_val;     // [2][kMaxLeafCTAs]
+  int* cand_row;   // [2][kMaxLeafCTAs]
+  T* cand_data;    // [2][kMaxLeafCTAs][kMaxLeafW]
+  T* rowj;         // [2][kMaxLeafW]
+};
+constexpr int kMaxLeafCTAs = 160;
+constexpr int kMaxLeafW = 64;
+template <typename T>
+int leaf_init();
+// Factor P[0:M, 0:ncols] (row-major, P = diagonal of the first column) with
+// partial pivoting; ipiv[j] = row_base + local pivot row.
+template <typename T>
+int launch_getf2_leaf(T* P, int64_t lda, int M, int ncols, int32_t* ipiv, int row_base, const LeafScratch<T>& scr,
+                      unsigned* bar, DevStatus* st, int info_base, double thr, long long spin, int max_ctas,
+                      cudaStream_t s);
+
+// ---- pivot batches: compose sequential swaps into (dst <- src) lists
+// batch: swaps (k0+i) <-> ipiv[k0+i] for i in [0, cnt), cnt <= kMaxBatch
+constexpr int kMaxBatch = 1024;
+struct PivotList {
+  int32_t* dst;  // [2*kMaxBatch]
+  int32_t* src;  // [2*kMaxBatch]
+  int32_t* m;    // [1]
+};
+int launch_pivot_compose(const int32_t* ipiv, int k0, int cnt, const PivotList& pl, cudaStream_t s);
+// Apply to columns [c_begin, c_end) minus [skip_begin, skip_end); optional
+// vector (rhs) and int permutation carried with the rows.
+template <typename T>
+int launch_pivot_apply(T* A, int64_t lda, int c_begin, int c_end, int skip_begin, int skip_end, const PivotList& pl,
+                       int max_m, double* rhs, int32_t* perm, cudaStream_t s);
+// Full permutation from an ipiv vector (single CTA, batched composition).
+int launch_ipiv_to_perm(const int32_t* ipiv, int n, int32_t* perm, int32_t* work, cudaStream_t s);
+
+// ---- triangular solves
+// B(m x ncols) <- L^{-1} B, L unit lower m x m (m <= 32), row-major
+template <typename T>
+int launch_trsm_llu_leaf(const T* L, int64_t ldl, T* B, int64_t ldb, int m, int ncols, cudaStream_t s);
+// single/multi right-hand side substitution with flags (persistent tickets)
+template <typename T>
+int launch_trsv(const T* LU, int64_t lda, int n, T* x, int upper, int* flags, unsigned* ticket, DevStatus* st,
+                long long spin, cudaStream_t s);
+
+// ---- residual / GEMV / generators
+struct ResidualAccum {  // non-negative doubles stored as ordered bit patterns
+  unsigned long long amax, anorm, bmax, xmax, rmax;
+};
+int launch_residual_f64(const double* A, int64_t lda, int n, const double* x, const double* b, double* r,
+                        ResidualAccum* acc, cudaStream_t s);
+int launch_gen_uniform(double* d, int64_t rows, int64_t cols, int64_t ld, uint64_t seed, uint64_t stream_id,
+                       cudaStream_t s);
+int launch_gather_perm(const double* b, const int32_t* perm, double* y, int n, cudaStream_t s);
+int launch_scatter_perm(const double* y, const int32_t* perm, double* b, int n, cudaStream_t s);
+int launch_iota(int32_t* p, int n, cudaStream_t s);
+
+}  // namespace lub

@@ -1,0 +1,452 @@
+// Host orchestration and C ABI (include/lu_b200.h).
+//
+// The reference drives the factorisation with Charm++ SDAG control flow per
+// block chare (lu.ci:31-370) and a per-PE BlockScheduler (scheduler.C).  On
+// one GPU that control collapses into a host loop over panel steps that
+// enqueues kernels on a stream:
+//   panel k     recursive getrf2: leaf getf2 kernels + laswp/TRSM/GEMM halves
+//   laswp       the panel's pivots applied to every other column, to b and to
+//               the row permutation (pivotBatch/applyTrailingPivots,
+//               lu.ci:92-123, lu.C:46-169)
+//   TRSM        U block row (factorAboveDiagBlock -> computeU, lu.ci:132-174)
+//   GEMM        one trailing update for the whole step (updateMatrix)
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace lub {
+
+// ---------------------------------------------------------------------------
+// tensor maps
+// ---------------------------------------------------------------------------
+typedef CUresult (*PFN_encodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static PFN_encodeTiled get_encode() {
+  static PFN_encodeTiled fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_encodeTiled>(p);
+  });
+  return fn;
+}
+
+int encode_tmap_2d(CUtensorMap* map, CUtensorMapDataType dtype, int elem_bytes, const void* base, uint64_t cols,
+                   uint64_t rows, uint64_t row_pitch_bytes, uint32_t box_cols, uint32_t box_rows,
+                   CUtensorMapSwizzle swizzle) {
+  PFN_encodeTiled enc = get_encode();
+  if (!enc) return LU_ERR_CUDA;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (row_pitch_bytes & 15)) return LU_ERR_ALIGN;
+  cuuint64_t gdim[2] = {cols, rows};
+  cuuint64_t gstride[1] = {row_pitch_bytes};
+  cuuint32_t box[2] = {box_cols, box_rows};
+  cuuint32_t estride[2] = {1, 1};
+  (void)elem_bytes;
+  CUresult r = enc(map, dtype, 2, const_cast<void*>(base), gdim, gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    fprintf(stderr, "[lu_b200] cuTensorMapEncodeTiled failed (%d)\n", (int)r);
+    return LU_ERR_CUDA;
+  }
+  return LU_OK;
+}
+
+// A row-major FP64 matrix with the two tensor maps the GEMM reads it by.
+struct MatF64 {
+  double* p = nullptr;
+  int64_t ld = 0, rows = 0, cols = 0;
+  CUtensorMap mapA, mapB;  // boxes 16x128 and 16x16, 128-byte swizzle
+  int init(double* ptr, int64_t r, int64_t c, int64_t ldd) {
+    p = ptr; rows = r; cols = c; ld = ldd;
+    LUB_TRY(encode_tmap_2d(&mapA, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, ptr, c, r, ld * 8, 16, 128,
+                           CU_TENSOR_MAP_SWIZZLE_128B));
+    LUB_TRY(encode_tmap_2d(&mapB, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, ptr, c, r, ld * 8, 16, 16,
+                           CU_TENSOR_MAP_SWIZZLE_128B));
+    return LU_OK;
+  }
+  double* at(int64_t r, int64_t c) const { return p + r * ld + c; }
+};
+
+static int g_init_status = -1000;
+static std::mutex g_init_mu;
+static int ensure_kernels_init() {
+  std::lock_guard<std::mutex> lk(g_init_mu);
+  if (g_init_status != -1000) return g_init_status;
+  int s = gemm_f64_init();
+  if (s == LU_OK) s = leaf_init<double>();
+  if (s == LU_OK) s = leaf_init<float>();
+  g_init_status = s;
+  return s;
+}
+
+}  // namespace lub
+
+using namespace lub;
+
+struct lu_handle_s {
+  lu_config cfg;
+  int device = 0;
+  int num_sms = 148;
+  // workspace (device)
+  DevStatus* st = nullptr;
+  unsigned* counters = nullptr;
+  int n_counters = 0;
+  int next_counter = 0;
+  LeafScratch<double> leaf64{};
+  LeafScratch<float> leaf32{};
+  PivotList plist{};
+  int32_t* perm = nullptr;
+  int32_t* perm_work = nullptr;
+  int* trsv_flags = nullptr;
+  unsigned* trsv_ticket = nullptr;
+  double* vec = nullptr;
+  double* vec2 = nullptr;
+  ResidualAccum* racc = nullptr;
+  ResidualAccum* racc_host = nullptr;
+  std::vector<void*> allocs;
+  size_t bytes = 0;
+  long long spin = 0;
+
+  template <typename T>
+  int alloc(T** p, size_t count) {
+    void* q = nullptr;
+    if (cudaMalloc(&q, std::max<size_t>(count * sizeof(T), 16)) != cudaSuccess) {
+      cudaGetLastError();
+      return LU_ERR_NOMEM;
+    }
+    allocs.push_back(q);
+    bytes += count * sizeof(T);
+    *p = static_cast<T*>(q);
+    return LU_OK;
+  }
+  unsigned* take_counter() {
+    if (next_counter >= n_counters) return nullptr;
+    return counters + next_counter++;
+  }
+};
+
+namespace {
+
+// even split of a column block, multiple of 16 when wide enough
+inline int split_w(int w) {
+  int h = w / 2;
+  int w1 = h >= 16 ? (h & ~15) : (h & ~1);
+  return std::max(w1, 2);
+}
+
+struct Ctx64 {
+  lu_handle h;
+  MatF64 A;
+  int32_t* ipiv;
+  int n;
+  cudaStream_t s;
+  double thr;
+};
+
+int pivots_apply_f64(Ctx64& c, int k0, int cnt, int c_begin, int c_end, int skip_b, int skip_e, double* rhs,
+                     int32_t* perm) {
+  for (int off = 0; off < cnt; off += 512) {
+    const int sub = std::min(512, cnt - off);
+    LUB_TRY(launch_pivot_compose(c.ipiv, k0 + off, sub, c.h->plist, c.s));
+    LUB_TRY(launch_pivot_apply<double>(c.A.p, c.A.ld, c_begin, c_end, skip_b, skip_e, c.h->plist, 2 * sub, rhs, perm,
+                                       c.s));
+  }
+  return LU_OK;
+}
+
+// C(rc, cc) [M x N] -= A(ra, ca) [M x K] * B(rb, cb) [K x N]
+int gemm64(Ctx64& c, const MatF64& Cm, int rc, int cc, const MatF64& Am, int ra, int ca, const MatF64& Bm, int rb,
+           int cb, int M, int N, int K) {
+  GemmArgs g;
+  g.a_row0 = ra; g.a_col0 = ca; g.b_row0 = rb; g.b_col0 = cb;
+  g.C = Cm.at(rc, cc); g.ldc = Cm.ld;
+  g.M = M; g.N = N; g.K = K;
+  g.st = c.h->st; g.spin = c.h->spin;
+  return launch_gemm_f64_sub(Am.mapA, Bm.mapB, g, c.s);
+}
+
+// B(r0.., cb..) [w x ncols] <- L^{-1} B, L = unit lower of Lm at (r0, r0)
+int trsm64(Ctx64& c, const MatF64& Lm, int r0, int w, const MatF64& Bm, int rb, int cb, int ncols) {
+  if (w <= 32) return launch_trsm_llu_leaf<double>(Lm.at(r0, r0), Lm.ld, Bm.at(rb, cb), Bm.ld, w, ncols, c.s);
+  const int w1 = split_w(w);
+  LUB_TRY(trsm64(c, Lm, r0, w1, Bm, rb, cb, ncols));
+  LUB_TRY(gemm64(c, Bm, rb + w1, cb, Lm, r0 + w1, r0, Bm, rb, cb, w - w1, ncols, w1));
+  return trsm64(c, Lm, r0 + w1, w - w1, Bm, rb + w1, cb, ncols);
+}
+
+// recursive panel factorisation of columns [c0, c0+w), rows [c0, n)
+int panel64(Ctx64& c, int c0, int w) {
+  const int M = c.n - c0;
+  if (w <= 32) {
+    unsigned* bar = c.h->take_counter();
+    if (!bar) return LU_ERR_NOMEM;
+    return launch_getf2_leaf<double>(c.A.at(c0, c0), c.A.ld, M, w, c.ipiv + c0, c0, c.h->leaf64, bar, c.h->st, c0,
+                                     c.thr, c.h->spin, c.h->num_sms, c.s);
+  }
+  const int w1 = split_w(w), w2 = w - w1;
+  LUB_TRY(panel64(c, c0, w1));
+  LUB_TRY(pivots_apply_f64(c, c0, w1, c0 + w1, c0 + w, 0, 0, nullptr, nullptr));
+  LUB_TRY(trsm64(c, c.A, c0, w1, c.A, c0, c0 + w1, w2));
+  LUB_TRY(gemm64(c, c.A, c0 + w1, c0 + w1, c.A, c0 + w1, c0, c.A, c0, c0 + w1, M - w1, w2, w1));
+  LUB_TRY(panel64(c, c0 + w1, w2));
+  return pivots_apply_f64(c, c0 + w1, w2, c0, c0 + w1, 0, 0, nullptr, nullptr);
+}
+
+int check_common(lu_handle h, const void* dA, int64_t lda) {
+  if (!h || !dA) return LU_ERR_ARG;
+  if (lda < h->cfg.n) return LU_ERR_ARG;
+  if ((lda & 1) || (reinterpret_cast<uintptr_t>(dA) & 15)) return LU_ERR_ALIGN;
+  return ensure_kernels_init();
+}
+
+int factor_f64(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double* rhs, cudaStream_t s) {
+  LUB_TRY(check_common(h, dA, lda));
+  if (!ipiv) return LU_ERR_ARG;
+  const int n = (int)h->cfg.n, b = h->cfg.block_size;
+  Ctx64 c;
+  c.h = h; c.ipiv = ipiv; c.n = n; c.s = s; c.thr = h->cfg.sing_threshold;
+  LUB_TRY(c.A.init(dA, n, n, lda));
+  LUB_CUDA(cudaMemsetAsync(h->st, 0, sizeof(DevStatus), s));
+  LUB_CUDA(cudaMemsetAsync(h->counters, 0, sizeof(unsigned) * h->n_counters, s));
+  h->next_counter = 0;
+  LUB_TRY(launch_iota(h->perm, n, s));
+  for (int k0 = 0; k0 < n; k0 += b) {
+    const int kw = std::min(b, n - k0);
+    LUB_TRY(panel64(c, k0, kw));
+    LUB_TRY(pivots_apply_f64(c, k0, kw, 0, n, k0, k0 + kw, rhs, h->perm));
+    const int rest = n - k0 - kw;
+    if (rest > 0) {
+      LUB_TRY(trsm64(c, c.A, k0, kw, c.A, k0, k0 + kw, rest));
+      LUB_TRY(gemm64(c, c.A, k0 + kw, k0 + kw, c.A, k0 + kw, k0, c.A, k0, k0 + kw, rest, rest, kw));
+    }
+  }
+  return LU_OK;
+}
+
+// x <- U^{-1} L^{-1} x (x already permuted)
+int solve_permuted_f64(lu_handle h, const double* LU, int64_t lda, double* x, cudaStream_t s) {
+  const int n = (int)h->cfg.n;
+  LUB_TRY(launch_trsv<double>(LU, lda, n, x, 0, h->trsv_flags, h->trsv_ticket, h->st, h->spin, s));
+  LUB_TRY(launch_trsv<double>(LU, lda, n, x, 1, h->trsv_flags, h->trsv_ticket, h->st, h->spin, s));
+  return LU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lu_config_default(lu_config* cfg, int64_t n, int32_t block_size) {
+  if (!cfg) return LU_ERR_ARG;
+  memset(cfg, 0, sizeof(*cfg));
+  cfg->n = n;
+  cfg->block_size = block_size;
+  cfg->pivot_batch = std::max(1, block_size / 4);
+  cfg->precision = LU_PREC_FP64;
+  cfg->lookahead = 0;
+  cfg->use_graph = 0;
+  cfg->ir_mode = LU_IR_CLASSIC;
+  cfg->ir_max_iter = 50;
+  cfg->sing_threshold = 0.0;
+  cfg->ir_target = 16.0;
+  cfg->spin_limit = 0;
+  return LU_OK;
+}
+
+size_t lu_workspace_bytes(const lu_config* cfg) {
+  if (!cfg) return 0;
+  const size_t n = (size_t)cfg->n;
+  size_t b = 0;
+  b += sizeof(DevStatus);
+  b += sizeof(unsigned) * (n / 2 + 1024);
+  b += 2 * kMaxLeafCTAs * (sizeof(double) + sizeof(int)) + 2 * kMaxLeafCTAs * kMaxLeafW * sizeof(double) +
+       2 * kMaxLeafW * sizeof(double);
+  b += 2 * kMaxLeafCTAs * (sizeof(float) + sizeof(int)) + 2 * kMaxLeafCTAs * kMaxLeafW * sizeof(float) +
+       2 * kMaxLeafW * sizeof(float);
+  b += sizeof(int32_t) * (4 * kMaxBatch + 1);
+  b += sizeof(int32_t) * 2 * n;
+  b += sizeof(int) * (n / 64 + 2) + sizeof(unsigned);
+  b += sizeof(double) * 2 * n;
+  b += sizeof(ResidualAccum);
+  return b;
+}
+
+int lu_create(const lu_config* cfg, lu_handle* out) {
+  if (!cfg || !out) return LU_ERR_ARG;
+  if (cfg->n <= 0 || cfg->n > (int64_t)1 << 30 || cfg->block_size < 2 || (cfg->block_size & 1)) return LU_ERR_ARG;
+  if (cfg->precision < LU_PREC_FP64 || cfg->precision > LU_PREC_FP16S) return LU_ERR_ARG;
+  LUB_TRY(ensure_kernels_init());
+  lu_handle h = new lu_handle_s();
+  h->cfg = *cfg;
+  cudaGetDevice(&h->device);
+  cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
+  h->spin = cfg->spin_limit > 0 ? cfg->spin_limit : (1LL << 24);
+  const int64_t n = cfg->n;
+  int s = LU_OK;
+  h->n_counters = (int)(n / 2 + 1024);  // one per leaf launch; leaves are >= 2 columns wide
+  if (s == LU_OK) s = h->alloc(&h->st, 1);
+  if (s == LU_OK) s = h->alloc(&h->counters, h->n_counters);
+  if (s == LU_OK) s = h->alloc(&h->leaf64.cand_val, 2 * kMaxLeafCTAs);
+  if (s == LU_OK) s = h->alloc(&h->leaf64.cand_row, 2 * kMaxLeafCTAs);
+  if (s == LU_OK) s = h->alloc(&h->leaf64.cand_data, 2 * kMaxLeafCTAs * kMaxLeafW);
+  if (s == LU_OK) s = h->alloc(&h->leaf64.rowj, 2 * kMaxLeafW);
+  if (s == LU_OK) s = h->alloc(&h->leaf32.cand_val, 2 * kMaxLeafCTAs);
+  if (s == LU_OK) s = h->alloc(&h->leaf32.cand_row, 2 * kMaxLeafCTAs);
+  if (s == LU_OK) s = h->alloc(&h->leaf32.cand_data, 2 * kMaxLeafCTAs * kMaxLeafW);
+  if (s == LU_OK) s = h->alloc(&h->leaf32.rowj, 2 * kMaxLeafW);
+  if (s == LU_OK) s = h->alloc(&h->plist.dst, 2 * kMaxBatch);
+  if (s == LU_OK) s = h->alloc(&h->plist.src, 2 * kMaxBatch);
+  if (s == LU_OK) s = h->alloc(&h->plist.m, 1);
+  if (s == LU_OK) s = h->alloc(&h->perm, n);
+  if (s == LU_OK) s = h->alloc(&h->perm_work, n);
+  if (s == LU_OK) s = h->alloc(&h->trsv_flags, n / 64 + 2);
+  if (s == LU_OK) s = h->alloc(&h->trsv_ticket, 1);
+  if (s == LU_OK) s = h->alloc(&h->vec, n);
+  if (s == LU_OK) s = h->alloc(&h->vec2, n);
+  if (s == LU_OK) s = h->alloc(&h->racc, 1);
+  if (s == LU_OK && cudaMallocHost(&h->racc_host, sizeof(ResidualAccum)) != cudaSuccess) s = LU_ERR_NOMEM;
+  if (s == LU_OK && cudaMemset(h->st, 0, sizeof(DevStatus)) != cudaSuccess) s = LU_ERR_CUDA;
+  if (s != LU_OK) {
+    lu_destroy(h);
+    return s;
+  }
+  *out = h;
+  return LU_OK;
+}
+
+int lu_destroy(lu_handle h) {
+  if (!h) return LU_ERR_ARG;
+  for (void* p : h->allocs) cudaFree(p);
+  if (h->racc_host) cudaFreeHost(h->racc_host);
+  delete h;
+  return LU_OK;
+}
+
+int lu_status(lu_handle h, void* stream) {
+  if (!h) return LU_ERR_ARG;
+  LUB_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  DevStatus st;
+  LUB_CUDA(cudaMemcpy(&st, h->st, sizeof(st), cudaMemcpyDeviceToHost));
+  if (st.code != 0) return st.code;
+  return st.info;
+}
+
+int lu_factor(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double* rhs, void* stream) {
+  if (!h) return LU_ERR_ARG;
+  if (h->cfg.precision != LU_PREC_FP64) return LU_ERR_UNSUPPORTED;
+  return factor_f64(h, dA, lda, ipiv, rhs, (cudaStream_t)stream);
+}
+
+int lu_solve(lu_handle h, const double* dLU, int64_t lda, const int32_t* ipiv, double* dB, int64_t ldb,
+             int64_t nrhs, int trans, void* stream) {
+  LUB_TRY(check_common(h, dLU, lda));
+  if (!ipiv || !dB || nrhs < 1 || ldb < nrhs) return LU_ERR_ARG;
+  if (trans != 0 || nrhs != 1) return LU_ERR_UNSUPPORTED;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int n = (int)h->cfg.n;
+  LUB_TRY(launch_ipiv_to_perm(ipiv, n, h->perm_work, nullptr, s));
+  LUB_TRY(launch_gather_perm(dB, h->perm_work, h->vec, n, s));
+  LUB_TRY(solve_permuted_f64(h, dLU, lda, h->vec, s));
+  LUB_CUDA(cudaMemcpyAsync(dB, h->vec, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  return LU_OK;
+}
+
+int lu_factor_solve(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double* db, void* stream) {
+  if (!h || !db) return LU_ERR_ARG;
+  if (h->cfg.precision != LU_PREC_FP64) return LU_ERR_UNSUPPORTED;
+  cudaStream_t s = (cudaStream_t)stream;
+  LUB_TRY(factor_f64(h, dA, lda, ipiv, db, s));
+  return solve_permuted_f64(h, dA, lda, db, s);
+}
+
+int lu_residual(lu_handle h, const double* dA, int64_t lda, const double* dx, const double* db,
+                lu_residual_info* out, void* stream) {
+  if (!h || !dA || !dx || !db || !out || lda < h->cfg.n) return LU_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int n = (int)h->cfg.n;
+  LUB_TRY(launch_residual_f64(dA, lda, n, dx, db, nullptr, h->racc, s));
+  LUB_CUDA(cudaMemcpyAsync(h->racc_host, h->racc, sizeof(ResidualAccum), cudaMemcpyDeviceToHost, s));
+  LUB_CUDA(cudaStreamSynchronize(s));
+  const ResidualAccum& a = *h->racc_host;
+  auto d = [](unsigned long long v) {
+    double x;
+    memcpy(&x, &v, 8);
+    return x;
+  };
+  const double eps = 2.220446049250313e-16, dn = (double)n;
+  out->amax = d(a.amax);
+  out->anorm = d(a.anorm);
+  out->bnorm = d(a.bmax);
+  out->xnorm = d(a.xmax);
+  out->rnorm = d(a.rmax);
+  out->r_ref = out->rnorm / ((out->amax * out->xnorm + out->bnorm) * dn * eps);
+  out->r_hpl = out->rnorm / ((out->anorm * out->xnorm + out->bnorm) * dn * eps);
+  return LU_OK;
+}
+
+int lu_refine_solve(lu_handle h, const double* dA, int64_t lda, const double* db, double* dx, lu_refine_info* info,
+                    void* stream) {
+  (void)h; (void)dA; (void)lda; (void)db; (void)dx; (void)info; (void)stream;
+  return LU_ERR_UNSUPPORTED;
+}
+
+int lu_adjoint(lu_handle h, const double* dLU, int64_t lda, const int32_t* ipiv, const double* dX, int64_t ldx,
+               const double* dW, int64_t ldw, int64_t nrhs, double* gradB, int64_t ldgb, double* gradA,
+               int64_t ldga, void* stream) {
+  (void)h; (void)dLU; (void)lda; (void)ipiv; (void)dX; (void)ldx; (void)dW; (void)ldw; (void)nrhs; (void)gradB;
+  (void)ldgb; (void)gradA; (void)ldga; (void)stream;
+  return LU_ERR_UNSUPPORTED;
+}
+
+int lu_batched_factor_solve(int32_t count, const int32_t* n, const int64_t* a_off, const int64_t* b_off, double* dA,
+                            double* db, int32_t* info, int32_t precision, void* dWork, size_t work_bytes,
+                            void* stream) {
+  (void)count; (void)n; (void)a_off; (void)b_off; (void)dA; (void)db; (void)info; (void)precision; (void)dWork;
+  (void)work_bytes; (void)stream;
+  return LU_ERR_UNSUPPORTED;
+}
+
+int lu_generate_uniform(double* d, int64_t rows, int64_t cols, int64_t ld, uint64_t seed, uint64_t stream_id,
+                        void* stream) {
+  if (!d || rows < 0 || cols < 0 || ld < cols) return LU_ERR_ARG;
+  return launch_gen_uniform(d, rows, cols, ld, seed, stream_id, (cudaStream_t)stream);
+}
+
+int lu_matgen_host(double* out, int64_t count, int32_t seed, int64_t skip) {
+  if (!out || count < 0 || skip < 0) return LU_ERR_ARG;
+  const int32_t MAXI = 0x7fffffff, A = 48271, Q = MAXI / A, R = MAXI % A;
+  int32_t cur = seed;
+  for (int64_t i = 0; i < skip + count; i++) {
+    cur = A * (cur % Q) - R * (cur / Q);
+    if (cur < 0) cur += MAXI;
+    if (i >= skip) out[i - skip] = (double)cur / MAXI - 0.5;
+  }
+  return LU_OK;
+}
+
+const char* lu_status_string(int status) {
+  if (status > 0) return "singular pivot (info = first failing column, 1-based)";
+  switch (status) {
+    case LU_OK: return "ok";
+    case LU_ERR_ARG: return "bad argument";
+    case LU_ERR_CUDA: return "CUDA error";
+    case LU_ERR_TIMEOUT: return "device-side wait timed out";
+    case LU_ERR_NONFINITE: return "non-finite value";
+    case LU_ERR_NOCONV: return "iterative refinement did not converge";
+    case LU_ERR_ALIGN: return "alignment requirement violated";
+    case LU_ERR_NOMEM: return "out of device memory";
+    case LU_ERR_UNSUPPORTED: return "unsupported configuration";
+    default: return "unknown status";
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,220 @@
+// Unblocked panel factorisation (getf2) of a tall, narrow column block.
+//
+// Restates the per-column loop of factorDiagBlock / factorBelowDiagBlock
+// (lu.ci:186-370) and its kernels:
+//   findMaxElm          lu.C:197-205   (strict '>', first row wins)
+//   MaxElm_max reducer  lu.C:207-218   (ties: lowest global row here; the
+//                                       reference's order is message-arrival
+//                                       dependent)
+//   swapLocal / pivotRowSwap            lu.C:172-177, lu.ci:302-323
+//   computeMultipliersAndFindColMax     lu.C:259-288 (true division, fused
+//                                       next-column update + candidate)
+//   updateLsubBlock (dger, offset 2)    lu.C:230-254
+//   singularity check                   lu.ci:339-341 (reported, not aborted)
+//
+// Design: a cooperative grid of G CTAs, each holding a contiguous range of
+// the panel's rows in shared memory for the whole launch (row pitch W+1 so a
+// warp walking one column touches distinct banks).  Per column: each CTA
+// publishes its candidate (|value|, row, the row's W values) and, if it owns
+// row j, that row; one bounded grid barrier; every CTA reduces the G
+// candidates (warp shuffles), takes the pivot row from the winner's slot,
+// swaps locally, scales and updates its rows, and computes its candidate for
+// the next column in the same pass.  Slots are double-buffered by column
+// parity, which is safe because a CTA cannot reach barrier j+2 before every
+// CTA has left barrier j+1.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace lub {
+namespace {
+
+constexpr int THREADS = 256;
+
+template <typename T>
+__device__ __forceinline__ bool cand_better(T v1, int r1, T v2, int r2) {
+  // (v1, r1) beats (v2, r2): valid and strictly larger, or equal and lower row
+  return r1 >= 0 && (r2 < 0 || v1 > v2 || (v1 == v2 && r1 < r2));
+}
+
+template <typename T>
+__device__ __forceinline__ void warp_argmax(T& v, int& r, int& w) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    T v2 = __shfl_xor_sync(0xffffffffu, v, o);
+    int r2 = __shfl_xor_sync(0xffffffffu, r, o);
+    int w2 = __shfl_xor_sync(0xffffffffu, w, o);
+    if (cand_better(v2, r2, v, r)) { v = v2; r = r2; w = w2; }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void block_argmax(T v, int r, T* s_v, int* s_r, T& out_v, int& out_r) {
+  int w = 0;
+  warp_argmax(v, r, w);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) { s_v[warp] = v; s_r[warp] = r; }
+  __syncthreads();
+  if (warp == 0) {
+    v = lane < THREADS / 32 ? s_v[lane] : T(0);
+    r = lane < THREADS / 32 ? s_r[lane] : -1;
+    warp_argmax(v, r, w);
+    if (lane == 0) { s_v[8] = v; s_r[8] = r; }
+  }
+  __syncthreads();
+  out_v = s_v[8];
+  out_r = s_r[8];
+}
+
+template <typename T, int W>
+__global__ void __launch_bounds__(THREADS, 1)
+getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int row_base, LeafScratch<T> scr,
+                  unsigned* bar, DevStatus* st, int info_base, double thr, long long spin) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int LD = W + 1;
+  T* a = reinterpret_cast<T*>(smem_raw);  // [R][LD]
+  T* urow = a + (size_t)R * LD;           // [W] pivot row
+  __shared__ T s_v[9];
+  __shared__ int s_r[9];
+  __shared__ int s_p, s_win;
+
+  const int G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x;
+  const int r_lo = cta * R;
+  const int r_hi = min(M, r_lo + R);
+  const int nr = r_hi - r_lo;
+
+  for (int idx = tid; idx < nr * ncols; idx += THREADS) {
+    const int r = idx / ncols, c = idx - r * ncols;
+    a[r * LD + c] = P[(int64_t)(r_lo + r) * lda + c];
+  }
+  __syncthreads();
+
+  // candidate of column 0 (findMaxElm(0, 0), lu.ci:266)
+  T cv = 0;
+  int cr = -1;
+  {
+    T bv = 0;
+    int br = -1;
+    for (int r = tid; r < nr; r += THREADS) {
+      T v = fabs(a[r * LD]);
+      if (v > bv) { bv = v; br = r_lo + r; }
+    }
+    block_argmax(bv, br, s_v, s_r, cv, cr);
+  }
+
+  for (int j = 0; j < ncols; j++) {
+    const int slot = j & 1;
+    // ---- publish candidate, its row, and row j if owned
+    if (tid < ncols) {
+      if (cr >= 0) scr.cand_data[((size_t)slot * kMaxLeafCTAs + cta) * kMaxLeafW + tid] = a[(cr - r_lo) * LD + tid];
+      if (j >= r_lo && j < r_hi) scr.rowj[slot * kMaxLeafW + tid] = a[(j - r_lo) * LD + tid];
+    }
+    if (tid == 0) {
+      scr.cand_val[slot * kMaxLeafCTAs + cta] = cv;
+      scr.cand_row[slot * kMaxLeafCTAs + cta] = cr;
+    }
+    __threadfence();
+    if (!grid_barrier(bar, (unsigned)(j + 1) * (unsigned)G, st, spin, 201)) return;
+
+    // ---- global argmax over the G candidates
+    if (tid < 32) {
+      T v = 0;
+      int r = -1, w = 0;
+      for (int q = tid; q < G; q += 32) {
+        T v2 = __ldcg(&scr.cand_val[slot * kMaxLeafCTAs + q]);
+        int r2 = __ldcg(&scr.cand_row[slot * kMaxLeafCTAs + q]);
+        if (cand_better(v2, r2, v, r)) { v = v2; r = r2; w = q; }
+      }
+      warp_argmax(v, r, w);
+      if (tid == 0) { s_p = r; s_win = w; }
+    }
+    __syncthreads();
+    const bool zero_col = s_p < 0;
+    const int p = zero_col ? j : s_p;
+    if (tid < ncols) {
+      urow[tid] = zero_col ? __ldcg(&scr.rowj[slot * kMaxLeafW + tid])
+                           : __ldcg(&scr.cand_data[((size_t)slot * kMaxLeafCTAs + s_win) * kMaxLeafW + tid]);
+    }
+    __syncthreads();
+    if (tid < ncols && p != j) {
+      if (p >= r_lo && p < r_hi) a[(p - r_lo) * LD + tid] = __ldcg(&scr.rowj[slot * kMaxLeafW + tid]);
+      if (j >= r_lo && j < r_hi) a[(j - r_lo) * LD + tid] = urow[tid];
+    }
+    const T piv = urow[j];
+    if (cta == 0 && tid == 0) {
+      ipiv[j] = row_base + p;
+      if (!(fabs((double)piv) > thr)) dev_singular(st, info_base + j + 1);
+    }
+    __syncthreads();
+
+    // ---- multipliers, rank-1 update of the remaining leaf columns, and the
+    //      candidate of column j+1 in the same pass
+    const bool do_scale = (piv != T(0)) && !isnan(piv);
+    const bool has_next = j + 1 < ncols;
+    T bv = 0;
+    int br = -1;
+    const int r_first = max(j + 1 - r_lo, 0);
+    for (int r = r_first + tid; r < nr; r += THREADS) {
+      T* ar = a + r * LD;
+      if (do_scale) {
+        const T l = ar[j] / piv;
+        ar[j] = l;
+        for (int c = j + 1; c < ncols; c++) ar[c] = fma(-l, urow[c], ar[c]);
+      }
+      if (has_next) {
+        T v = fabs(ar[j + 1]);
+        if (v > bv) { bv = v; br = r_lo + r; }
+      }
+    }
+    block_argmax(bv, br, s_v, s_r, cv, cr);
+  }
+
+  for (int idx = tid; idx < nr * ncols; idx += THREADS) {
+    const int r = idx / ncols, c = idx - r * ncols;
+    P[(int64_t)(r_lo + r) * lda + c] = a[r * LD + c];
+  }
+}
+
+template <typename T>
+constexpr int leaf_w() { return sizeof(T) == 8 ? 32 : 64; }
+
+template <typename T>
+size_t leaf_smem(int R) { return (size_t)R * (leaf_w<T>() + 1) * sizeof(T) + leaf_w<T>() * sizeof(T); }
+
+}  // namespace
+
+template <typename T>
+int leaf_init() {
+  LUB_CUDA(cudaFuncSetAttribute(getf2_leaf_kernel<T, leaf_w<T>()>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                220 * 1024));
+  return LU_OK;
+}
+
+template <typename T>
+int launch_getf2_leaf(T* P, int64_t lda, int M, int ncols, int32_t* ipiv, int row_base, const LeafScratch<T>& scr,
+                      unsigned* bar, DevStatus* st, int info_base, double thr, long long spin, int max_ctas,
+                      cudaStream_t s) {
+  constexpr int W = leaf_w<T>();
+  if (M <= 0 || ncols <= 0) return LU_OK;
+  if (ncols > W) return LU_ERR_ARG;
+  // rows per CTA: enough CTAs to spread the panel, capped by the SM count
+  // and by shared memory (R * (W+1) * sizeof(T) <= ~216 KB)
+  const int max_rows = (int)((216 * 1024 - W * sizeof(T)) / ((W + 1) * sizeof(T)));
+  int G = std::min(std::max(ceil_div(M, 256), 1), std::min(max_ctas, kMaxLeafCTAs));
+  int R = ceil_div(M, G);
+  if (R > max_rows) return LU_ERR_UNSUPPORTED;
+  G = ceil_div(M, R);
+  size_t smem = leaf_smem<T>(R);
+  void* args[] = {&P, &lda, &M, &ncols, &R, &ipiv, &row_base, const_cast<LeafScratch<T>*>(&scr), &bar, &st,
+                  &info_base, &thr, &spin};
+  LUB_CUDA(cudaLaunchCooperativeKernel((const void*)getf2_leaf_kernel<T, W>, dim3(G), dim3(THREADS), args, smem, s));
+  return LU_OK;
+}
+
+template int leaf_init<double>();
+template int leaf_init<float>();
+template int launch_getf2_leaf<double>(double*, int64_t, int, int, int32_t*, int, const LeafScratch<double>&,
+                                       unsigned*, DevStatus*, int, double, long long, int, cudaStream_t);
+template int launch_getf2_leaf<float>(float*, int64_t, int, int, int32_t*, int, const LeafScratch<float>&,
+                                      unsigned*, DevStatus*, int, double, long long, int, cudaStream_t);
+
+}  // namespace lub

@@ -1,0 +1,188 @@
+// Row interchanges (laswp) for a batch of pivots.
+//
+// The reference turns each batch of recorded pivots into permutation cycles
+// (recordPivot / announceAgglomeratedPivots, lu.C:305-352) and every block
+// applies them to its rows and to b (sendPendingPivots / applySwap,
+// lu.C:46-169).  Here a batch of sequential swaps (k0+i) <-> p_i, p_i >=
+// k0+i, is composed on the device into a simultaneous assignment
+// row[dst] <- row[src] over the affected rows, then applied to column strips
+// with every source read into shared memory before any destination is
+// written (one read and one write per moved row segment, all independent).
+//
+// Composition (parallel, O(cnt^2) comparisons in shared memory):
+//   c_i   = content of position k0+i just before swap i
+//         = c_{a(i)} if a(i) = last i' < i with p_{i'} = k0+i exists, else k0+i
+//           (resolved by pointer jumping);
+//   final(k0+i) = c_{b(i)} if b(i) = last i' < i with p_{i'} = p_i exists,
+//                 else p_i;
+//   final(x) for x = p_i >= k0+cnt, i the last swap touching x: c_i.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace lub {
+namespace {
+
+// Computes dst/src lists in shared memory; returns m (same in all threads).
+__device__ int compose_batch(const int32_t* ipiv, int k0, int cnt, int* p, int* nxt, int* lb, int* dst, int* src,
+                             int* s_m) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int i = tid; i < cnt; i += nt) p[i] = ipiv[k0 + i];
+  if (tid == 0) *s_m = 0;
+  __syncthreads();
+  for (int i = tid; i < cnt; i += nt) {
+    int la = -1, lbi = -1;
+    const int me = k0 + i, pi = p[i];
+    for (int q = 0; q < i; q++) {
+      const int pq = p[q];
+      if (pq == me) la = q;
+      if (pq == pi) lbi = q;
+    }
+    nxt[i] = la < 0 ? i : la;
+    lb[i] = lbi;
+  }
+  __syncthreads();
+  for (int span = 1; span < cnt; span <<= 1) {
+    int tmp[4];
+    int k = 0;
+    for (int i = tid; i < cnt && k < 4; i += nt, k++) tmp[k] = nxt[nxt[i]];
+    __syncthreads();
+    k = 0;
+    for (int i = tid; i < cnt && k < 4; i += nt, k++) nxt[i] = tmp[k];
+    __syncthreads();
+  }
+  // nxt[i] = root; c_i = k0 + root
+  for (int i = tid; i < cnt; i += nt) {
+    const int me = k0 + i, pi = p[i];
+    const int s = lb[i] >= 0 ? k0 + nxt[lb[i]] : pi;
+    if (s != me) {
+      int o = atomicAdd(s_m, 1);
+      dst[o] = me;
+      src[o] = s;
+    }
+    if (pi >= k0 + cnt) {
+      bool last = true;
+      for (int q = i + 1; q < cnt; q++)
+        if (p[q] == pi) { last = false; break; }
+      if (last) {
+        int o = atomicAdd(s_m, 1);
+        dst[o] = pi;
+        src[o] = k0 + nxt[i];
+      }
+    }
+  }
+  __syncthreads();
+  return *s_m;
+}
+
+__global__ void __launch_bounds__(1024) pivot_compose_kernel(const int32_t* ipiv, int k0, int cnt, PivotList pl) {
+  __shared__ int p[kMaxBatch], nxt[kMaxBatch], lb[kMaxBatch];
+  __shared__ int dst[2 * kMaxBatch], src[2 * kMaxBatch];
+  __shared__ int s_m;
+  const int m = compose_batch(ipiv, k0, cnt, p, nxt, lb, dst, src, &s_m);
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    pl.dst[i] = dst[i];
+    pl.src[i] = src[i];
+  }
+  if (threadIdx.x == 0) *pl.m = m;
+}
+
+template <typename T, int CS>
+__global__ void __launch_bounds__(256) pivot_apply_kernel(T* A, int64_t lda, int c_begin, int c_end, int skip_begin,
+                                                          int skip_end, PivotList pl, double* rhs, int32_t* perm) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* buf = reinterpret_cast<T*>(smem_raw);
+  const int m = *pl.m;
+  const int tid = threadIdx.x;
+  const int c0 = c_begin + blockIdx.x * CS;
+  const bool strip_live = c0 < c_end && !(c0 >= skip_begin && c0 + CS <= skip_end);
+  if (strip_live && m > 0) {
+    for (int idx = tid; idx < m * CS; idx += blockDim.x) {
+      const int i = idx / CS, c = idx - i * CS, col = c0 + c;
+      if (col < c_end && (col < skip_begin || col >= skip_end)) buf[idx] = A[(int64_t)pl.src[i] * lda + col];
+    }
+    __syncthreads();
+    for (int idx = tid; idx < m * CS; idx += blockDim.x) {
+      const int i = idx / CS, c = idx - i * CS, col = c0 + c;
+      if (col < c_end && (col < skip_begin || col >= skip_end)) A[(int64_t)pl.dst[i] * lda + col] = buf[idx];
+    }
+  }
+  if (blockIdx.x == 0 && m > 0 && (rhs || perm)) {
+    __syncthreads();
+    double* vb = reinterpret_cast<double*>(smem_raw);
+    int32_t* pb = reinterpret_cast<int32_t*>(vb + m);
+    for (int i = tid; i < m; i += blockDim.x) {
+      if (rhs) vb[i] = rhs[pl.src[i]];
+      if (perm) pb[i] = perm[pl.src[i]];
+    }
+    __syncthreads();
+    for (int i = tid; i < m; i += blockDim.x) {
+      if (rhs) rhs[pl.dst[i]] = vb[i];
+      if (perm) perm[pl.dst[i]] = pb[i];
+    }
+  }
+}
+
+// perm <- iota, then all pivot batches of 256 composed and applied in order.
+__global__ void __launch_bounds__(1024) ipiv_to_perm_kernel(const int32_t* ipiv, int n, int32_t* perm, int32_t* work) {
+  __shared__ int p[256], nxt[256], lb[256];
+  __shared__ int dst[512], src[512];
+  __shared__ int vals[512];
+  __shared__ int s_m;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = i;
+  __syncthreads();
+  for (int k0 = 0; k0 < n; k0 += 256) {
+    const int cnt = min(256, n - k0);
+    const int m = compose_batch(ipiv, k0, cnt, p, nxt, lb, dst, src, &s_m);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) vals[i] = perm[src[i]];
+    __syncthreads();
+    for (int i = threadIdx.x; i < m; i += blockDim.x) perm[dst[i]] = vals[i];
+    __syncthreads();
+  }
+}
+
+template <typename T>
+constexpr int apply_cs() { return 128 / (int)sizeof(T); }  // 128-byte row segments
+
+}  // namespace
+
+int launch_pivot_compose(const int32_t* ipiv, int k0, int cnt, const PivotList& pl, cudaStream_t s) {
+  if (cnt <= 0) return LU_OK;
+  if (cnt > kMaxBatch) return LU_ERR_ARG;
+  pivot_compose_kernel<<<1, 1024, 0, s>>>(ipiv, k0, cnt, pl);
+  LUB_LAUNCH_CHECK();
+  return LU_OK;
+}
+
+template <typename T>
+int launch_pivot_apply(T* A, int64_t lda, int c_begin, int c_end, int skip_begin, int skip_end, const PivotList& pl,
+                       int max_m, double* rhs, int32_t* perm, cudaStream_t s) {
+  constexpr int CS = apply_cs<T>();
+  if (c_end <= c_begin && !rhs && !perm) return LU_OK;
+  size_t smem = std::max((size_t)max_m * CS * sizeof(T), (size_t)max_m * (sizeof(double) + sizeof(int32_t)));
+  if (smem > 200 * 1024) return LU_ERR_ARG;
+  int strips = std::max(1, ceil_div(std::max(c_end - c_begin, 0), CS));
+  if (smem > 48 * 1024) {
+    static bool attr_set = false;
+    if (!attr_set) {
+      LUB_CUDA(cudaFuncSetAttribute(pivot_apply_kernel<T, CS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    200 * 1024));
+      attr_set = true;
+    }
+  }
+  pivot_apply_kernel<T, CS><<<strips, 256, smem, s>>>(A, lda, c_begin, c_end, skip_begin, skip_end, pl, rhs, perm);
+  LUB_LAUNCH_CHECK();
+  return LU_OK;
+}
+
+int launch_ipiv_to_perm(const int32_t* ipiv, int n, int32_t* perm, int32_t* work, cudaStream_t s) {
+  ipiv_to_perm_kernel<<<1, 1024, 0, s>>>(ipiv, n, perm, work);
+  LUB_LAUNCH_CHECK();
+  return LU_OK;
+}
+
+template int launch_pivot_apply<double>(double*, int64_t, int, int, int, int, const PivotList&, int, double*,
+                                        int32_t*, cudaStream_t);
+template int launch_pivot_apply<float>(float*, int64_t, int, int, int, int, const PivotList&, int, double*,
+                                       int32_t*, cudaStream_t);
+
+}  // namespace lub

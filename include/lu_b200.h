@@ -1,0 +1,196 @@
+/*
+ * lu_b200.h — C ABI of the B200-native dense LU solver (charmlu_b200).
+ *
+ * Drop-in for the factor-then-solve path of charmlu.  charmlu exposes that
+ * path as a Charm++ chare API plus a command line, not as a C ABI:
+ *   LUSolver(LUConfig, CkCallback)            benchmark.C:231-240, driver.ci:9-15
+ *   LUBlk::startup(LUConfig, ..., callbacks)   lu.ci:467-494
+ *   LUBlk::factor()                            lu.ci:31-42
+ *   LUBlk::forwardSolve()/backwardSolve()      lu.ci:387-436
+ *   BenchmarkLUBlk::startValidation() + LUSolver::calcScaledResidual
+ *                                              benchmark.C:462-573, 385-400
+ *   LUConfig {matrixSize, blockSize, pivotBatchSize, memThreshold, ...}
+ *                                              luConfig.h:8-62
+ * Each entry point below names the reference interface it replaces.
+ *
+ * Conventions
+ *  - Matrices are ROW-MAJOR with a leading dimension (the reference stores
+ *    every block row-major, lu.h:151-153).  Device pointers are cudaMalloc'd
+ *    memory of the current device; the caller owns them.
+ *  - Pivots are LAPACK-style 0-based global rows: ipiv[k] is the row swapped
+ *    with row k at step k (the reference's recordPivot(k, pivot.loc),
+ *    lu.ci:329).
+ *  - Every call is asynchronous on the given stream (a cudaStream_t passed
+ *    as void*; NULL = legacy default stream).  A call returns LU_OK or a
+ *    negative argument/launch error immediately; the numerical status
+ *    (singular column, device wait timeout, non-convergence) is read with
+ *    lu_status(), which synchronises the stream.  charmlu aborts instead
+ *    (CkAbort at lu.ci:339-341, CkExit at benchmark.C:143-147).
+ *  - A handle is not re-entrant: one call sequence at a time per handle.
+ *  - Alignment: base pointers 16-byte aligned; lda even for FP64 (the row
+ *    pitch must be a multiple of 16 bytes for the TMA tensor maps).
+ */
+#ifndef LU_B200_H
+#define LU_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LU_API __attribute__((visibility("default")))
+#else
+#define LU_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define LU_OK               0   /* >0: 1-based first column whose pivot failed the singularity test */
+#define LU_ERR_ARG         -1   /* bad argument (the reference's CkExit on bad config, benchmark.C:143-147) */
+#define LU_ERR_CUDA        -2   /* CUDA runtime/launch error */
+#define LU_ERR_TIMEOUT     -3   /* a bounded device-side wait gave up */
+#define LU_ERR_NONFINITE   -4   /* non-finite input or pivot */
+#define LU_ERR_NOCONV      -5   /* iterative refinement did not reach the residual target */
+#define LU_ERR_ALIGN       -6   /* pointer / leading-dimension alignment violated */
+#define LU_ERR_NOMEM       -7   /* workspace allocation failed */
+#define LU_ERR_UNSUPPORTED -8   /* configuration not supported by this build */
+
+/* ---- precision of the factorisation ---------------------------------- */
+#define LU_PREC_FP64   0   /* the reference's arithmetic (all FP64) */
+#define LU_PREC_BF16   1   /* FP32 panel/TRSM, BF16 tensor-core trailing update, FP64 refinement */
+#define LU_PREC_FP16S  2   /* as BF16 but FP16 operands with per-tile scaling */
+
+/* ---- refinement mode --------------------------------------------------- */
+#define LU_IR_CLASSIC  0   /* classical iterative refinement, GMRES-IR fallback on stagnation */
+#define LU_IR_GMRES    1   /* GMRES-IR from the start */
+
+/* Replaces LUConfig (luConfig.h:8-62).  Fields the reference uses for its
+ * distributed runtime (map, PE tiles, memThreshold, mcastMgrGID) have no
+ * meaning on one GPU; memThreshold is accepted by the CLI and ignored. */
+typedef struct lu_config {
+  int64_t n;               /* matrixSize */
+  int32_t block_size;      /* blockSize: panel width b (any even value >= 2) */
+  int32_t pivot_batch;     /* pivotBatchSize (default b/4, benchmark.C:98); swaps are applied per panel here */
+  int32_t precision;       /* LU_PREC_* */
+  int32_t lookahead;       /* 1 = overlap panel k+1 with trailing update k (two streams) */
+  int32_t use_graph;       /* 1 = capture the schedule once per (n, b) as a CUDA graph and replay it */
+  int32_t ir_mode;         /* LU_IR_* (mixed precision only) */
+  int32_t ir_max_iter;     /* refinement iteration cap */
+  int32_t reserved;
+  double  sing_threshold;  /* |u_jj| <= threshold sets info; the reference aborts at 100*eps (lu.ci:339) */
+  double  ir_target;       /* refinement stops when r_hpl < ir_target (default 16) */
+  int64_t spin_limit;      /* bounded-wait iteration cap for cross-CTA waits (0 = default) */
+} lu_config;
+
+typedef struct lu_handle_s* lu_handle;
+
+/* Residual report (benchmark.C:385-400, 476-573). */
+typedef struct lu_residual_info {
+  double amax;     /* max |a_ij| — the reference's "|A|inf" (benchmark.C:476-483) */
+  double anorm;    /* ||A||inf, max row sum */
+  double bnorm;    /* ||b||inf */
+  double xnorm;    /* ||x||inf */
+  double rnorm;    /* ||b - Ax||inf */
+  double r_ref;    /* rnorm / ((amax*xnorm + bnorm) * n * eps) — reference form, benchmark.C:390 */
+  double r_hpl;    /* rnorm / ((anorm*xnorm + bnorm) * n * eps) — HPL form */
+} lu_residual_info;
+
+/* Refinement report. */
+typedef struct lu_refine_info {
+  int32_t iterations;        /* classical IR iterations taken */
+  int32_t gmres_iterations;  /* inner GMRES iterations (0 if not used) */
+  int32_t used_gmres;        /* 1 if GMRES-IR ran */
+  int32_t status;            /* LU_OK or LU_ERR_NOCONV */
+  double  r_hpl;             /* final scaled residual */
+  double  r_hpl_initial;     /* scaled residual of the low-precision solve */
+} lu_refine_info;
+
+/* Fill *cfg with defaults for order n and block size b (LUConfig defaults,
+ * benchmark.C:91-134). */
+LU_API int lu_config_default(lu_config* cfg, int64_t n, int32_t block_size);
+
+/* Create / destroy a solver handle on the current device; allocates the
+ * handle's workspace (candidate slots, barrier counters, pivot lists).
+ * Replaces LUSolver construction + LUBlk::startup (benchmark.C:258-294,
+ * lu.ci:467-494). */
+LU_API int lu_create(const lu_config* cfg, lu_handle* out);
+LU_API int lu_destroy(lu_handle h);
+/* Device workspace bytes the handle holds (precision-dependent). */
+LU_API size_t lu_workspace_bytes(const lu_config* cfg);
+
+/* Synchronise `stream` and return the numerical status of the last call
+ * sequence on h: LU_OK, >0 singular column (1-based), or LU_ERR_*. */
+LU_API int lu_status(lu_handle h, void* stream);
+
+/* FP64 LU with partial pivoting in place: P A = L U, L unit lower.
+ * Replaces LUBlk::factor() (lu.ci:31-42) and its kernels (lu.C:26-352).
+ *   dA   : n x n row-major, lda >= n, overwritten with L\U
+ *   ipiv : n int32, 0-based global pivot rows
+ *   rhs  : optional n-vector permuted with the rows (the reference carries
+ *          b through the swaps, lu.h:66, lu.C:166-177), may be NULL */
+LU_API int lu_factor(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double* rhs, void* stream);
+
+/* Solve with stored factors.  trans = 0: A X = B (forwardSolve /
+ * backwardSolve, lu.ci:387-436, applying P first); trans = 1: A^T X = B
+ * (the adjoint; no reference counterpart).  B is n x nrhs row-major, ldb >=
+ * nrhs, overwritten by X. */
+LU_API int lu_solve(lu_handle h, const double* dLU, int64_t lda, const int32_t* ipiv,
+             double* dB, int64_t ldb, int64_t nrhs, int trans, void* stream);
+
+/* Time-to-solution entry: factor A and solve A x = b in one call, b
+ * overwritten by x.  This is the span the reference times
+ * (benchmark.C:243 -> 344: factor() then forwardSolve()). */
+LU_API int lu_factor_solve(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double* db, void* stream);
+
+/* Scaled residual of x against the ORIGINAL A and b (dA must hold A, not
+ * its factors).  Replaces startValidation/recvXvec/sumBvec/calcResiduals/
+ * calcScaledResidual (benchmark.C:462-573, 385-400).  Synchronises. */
+LU_API int lu_residual(lu_handle h, const double* dA, int64_t lda, const double* dx, const double* db,
+                lu_residual_info* out, void* stream);
+
+/* Mixed-precision solve (no reference counterpart): factor a low-precision
+ * working copy of A (h's precision), then refine x in FP64 against the
+ * untouched FP64 A until r_hpl < cfg.ir_target (classical IR, GMRES-IR as
+ * fallback).  dA is read only; db is read only; dx receives x. */
+LU_API int lu_refine_solve(lu_handle h, const double* dA, int64_t lda, const double* db, double* dx,
+                    lu_refine_info* info, void* stream);
+
+/* Adjoint of X = A^{-1} B (no reference counterpart).  Given the factors
+ * of A (from lu_factor), X (n x nrhs) and the upstream gradient W = dL/dX,
+ * computes lambda = A^{-T} W into gradB and grad_A = -lambda X^T into gradA
+ * (n x n, row-major, ldga).  gradA may be NULL. */
+LU_API int lu_adjoint(lu_handle h, const double* dLU, int64_t lda, const int32_t* ipiv,
+               const double* dX, int64_t ldx, const double* dW, int64_t ldw, int64_t nrhs,
+               double* gradB, int64_t ldgb, double* gradA, int64_t ldga, void* stream);
+
+/* Batched factor+solve of many independent systems of uneven order in one
+ * persistent launch (no reference counterpart).  System i has order n[i],
+ * its matrix at dA + a_off[i] (row-major, lda = n[i]) and right-hand side
+ * at db + b_off[i] (overwritten by x).  precision LU_PREC_FP64, or
+ * LU_PREC_BF16 meaning FP32 factors plus one FP64 refinement step (then
+ * dA must stay intact: factors go to the handle-free scratch dWork of
+ * 4*sum(n^2) bytes).  info[i] receives each system's status.  All arrays
+ * are device memory. */
+LU_API int lu_batched_factor_solve(int32_t count, const int32_t* n, const int64_t* a_off,
+                            const int64_t* b_off, double* dA, double* db, int32_t* info,
+                            int32_t precision, void* dWork, size_t work_bytes, void* stream);
+
+/* Generators (device).  Counter-based uniform[-0.5,0.5): element (i, j)
+ * of stream s is a pure function of (seed, s, i*cols + j), identical to
+ * the CPU oracle's.  The reference generates A per block from Charm++'s
+ * CrnDouble (benchmark.C:436-452), which is not reproducible here. */
+LU_API int lu_generate_uniform(double* d, int64_t rows, int64_t cols, int64_t ld, uint64_t seed,
+                        uint64_t stream_id, void* stream);
+/* The reference's b generator MatGen (benchmark.C:28-74, 455-460):
+ * minimal-standard LCG, seed 9934835 by default.  Host-side. */
+LU_API int lu_matgen_host(double* out, int64_t count, int32_t seed, int64_t skip);
+
+/* Message for a status code. */
+LU_API const char* lu_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LU_B200_H */

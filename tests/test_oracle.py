@@ -1,0 +1,103 @@
+"""CPU tests: the oracle against LAPACK, the reference's known answers and the
+committed golden fixtures."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "lu_golden.npz"))
+
+
+def test_matgen_known_answer():
+    # minimal standard with multiplier 48271 (benchmark.C:28-74): seed 1,
+    # 10000th draw is 399268537 (the published known answer)
+    _, ints = oracle.matgen(10000, seed=1)
+    assert ints[-1] == 399268537
+    assert int(GOLD["minstd_seed1_10000th"][0]) == 399268537
+
+
+def test_matgen_values_and_skip():
+    v, ints = oracle.matgen(16, seed=9934835)
+    np.testing.assert_array_equal(ints, GOLD["matgen_9934835_first16_int"])
+    np.testing.assert_array_equal(v, GOLD["matgen_9934835_first16"])
+    # genVec skips the draws of earlier blocks (benchmark.C:455-460)
+    v8, _ = oracle.matgen(8, seed=9934835, skip=8)
+    np.testing.assert_array_equal(v8, v[8:])
+    assert np.all(v >= -0.5) and np.all(v <= 0.5)
+
+
+def test_generator_range_and_determinism():
+    a = oracle.gen_uniform(100000, 42, 0)
+    assert a.min() >= -0.5 and a.max() < 0.5
+    assert abs(a.mean()) < 0.01
+    np.testing.assert_array_equal(a[1000:1010], oracle.gen_uniform(10, 42, 0, offset=1000))
+    assert not np.array_equal(a[:10], oracle.gen_uniform(10, 42, 1))
+
+
+@pytest.mark.parametrize("key", [k[:-5] for k in GOLD.files if k.endswith("_ipiv")])
+def test_oracle_matches_golden(key):
+    n, b = (int(s[1:]) for s in key.split("_"))
+    A = oracle.gen_matrix(n, 42)
+    rhs = oracle.gen_vector(n, 42)
+    np.testing.assert_array_equal(A.ravel()[:4], GOLD[key + "_a00"])
+    x, LU, ipiv, margin, info = oracle.solve(A, rhs, b=b)
+    assert info == 0
+    np.testing.assert_array_equal(ipiv, GOLD[key + "_ipiv"])
+    np.testing.assert_allclose(x, GOLD[key + "_x"], rtol=0, atol=1e-12 * np.abs(x).max())
+    if key + "_lu" in GOLD.files:
+        np.testing.assert_allclose(LU, GOLD[key + "_lu"], rtol=0, atol=1e-13 * np.abs(LU).max())
+
+
+@pytest.mark.parametrize("n,b", [(48, 12), (200, 16), (513, 64), (1024, 128)])
+def test_oracle_pivots_match_lapack(n, b):
+    import scipy.linalg as sl
+    A = oracle.gen_matrix(n, 7)
+    LU, ipiv, _, margin, info = oracle.lu_factor(A, b=b)
+    lu_l, piv_l = sl.lu_factor(A)
+    ok = margin > 1e-10  # near-ties excluded (rounding order may flip them)
+    assert np.array_equal(piv_l[ok], ipiv[ok])
+    assert np.abs(lu_l - LU).max() / np.abs(LU).max() < 1e-12
+
+
+def test_oracle_loops_equal_blas_mode():
+    A = oracle.gen_matrix(96, 3)
+    LU1, p1, _, _, _ = oracle.lu_factor(A, b=32, blas=True)
+    LU2, p2, _, _, _ = oracle.lu_factor(A, b=32, blas=False)
+    np.testing.assert_array_equal(p1, p2)
+    assert np.abs(LU1 - LU2).max() < 1e-13 * np.abs(LU1).max()
+
+
+@pytest.mark.parametrize("n,b", [(48, 48), (48, 24), (48, 16), (48, 12), (32, 8), (32, 4), (512, 128), (1024, 64)])
+def test_oracle_residual_contract(n, b):
+    """test_lu.pl passes a configuration when 'residual = X' has X < 16."""
+    A = oracle.gen_matrix(n, 42)
+    rhs = oracle.gen_vector(n, 42)
+    x, *_ = oracle.solve(A, rhs, b=b)
+    r = oracle.residual(A, x, rhs)
+    assert r["r_ref"] < 16 and r["r_hpl"] < 16
+    assert r["r_hpl"] <= r["r_ref"]
+
+
+def test_oracle_singular_reports_info():
+    A = oracle.gen_matrix(64, 5)
+    A[:, 10] = 0.0
+    LU, ipiv, _, _, info = oracle.lu_factor(A, b=16)
+    assert info == 11
+    A2 = oracle.gen_matrix(64, 5)
+    A2[20] = A2[3]  # duplicate row -> exact or near-zero pivot later
+    _, _, _, _, info2 = oracle.lu_factor(A2, b=16, sing_threshold=oracle.SING_REF)
+    assert info2 > 0
+
+
+def test_oracle_apply_pivots_roundtrip():
+    n = 300
+    A = oracle.gen_matrix(n, 9)
+    rhs = oracle.gen_vector(n, 9)
+    LU, ipiv, rp, _, _ = oracle.lu_factor(A, b=64, rhs=rhs)
+    np.testing.assert_array_equal(oracle.apply_pivots(rhs, ipiv), rp)
+    L = np.tril(LU, -1) + np.eye(n)
+    U = np.triu(LU)
+    PA = oracle.apply_pivots(A, ipiv)
+    assert np.abs(L @ U - PA).max() < 1e-12
