@@ -184,6 +184,19 @@ class LUSolver:
                "lu_residual")
         return {k: getattr(info, k) for k, _ in info._fields_}
 
+    def profile(self, enable=True):
+        """Bracket every phase of later calls with CUDA events (lu_profile)."""
+        _check(self._L.lu_profile(self._h, int(bool(enable))), "lu_profile")
+
+    def phase_times(self):
+        """{phase: (ms, calls, flops)} since the last call (synchronises)."""
+        n = len(_lib.PHASES)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_int64 * n)()
+        fl = (ctypes.c_double * n)()
+        _check(self._L.lu_phase_times(self._h, ms, cnt, fl), "lu_phase_times")
+        return {p: (ms[i], int(cnt[i]), fl[i]) for i, p in enumerate(_lib.PHASES)}
+
     def refine_solve(self, A, b, x=None, stream=None):
         """Mixed-precision factor + FP64 iterative refinement (A, b untouched)."""
         lda = self._check_matrix(A)
@@ -194,6 +207,11 @@ class LUSolver:
         _check(self._L.lu_refine_solve(self._h, _ptr(A), lda, _ptr(b), _ptr(x), ctypes.byref(info),
                                        _stream(stream)), "lu_refine_solve")
         return x, {k: getattr(info, k) for k, _ in info._fields_}
+
+
+def launch_count():
+    """Kernels liblu_b200 has launched since it was loaded."""
+    return int(_lib.load().lu_launch_count())
 
 
 def generate_uniform(rows, cols, seed=42, stream_id=0, device="cuda", out=None):

@@ -20,7 +20,9 @@ EXPORTS = [
     "lu_config_default", "lu_create", "lu_destroy", "lu_workspace_bytes", "lu_status", "lu_factor",
     "lu_solve", "lu_factor_solve", "lu_residual", "lu_refine_solve", "lu_adjoint",
     "lu_batched_factor_solve", "lu_generate_uniform", "lu_matgen_host", "lu_status_string",
+    "lu_profile", "lu_phase_times", "lu_launch_count",
 ]
+PHASES = ["panel", "laswp", "trsm", "gemm", "gemm_inner", "solve", "other"]
 
 
 class LuConfig(ctypes.Structure):
@@ -71,6 +73,9 @@ def load():
         "lu_generate_uniform": ([P, i64, i64, i64, u64, u64, P], ctypes.c_int),
         "lu_matgen_host": ([P, i64, i32, i64], ctypes.c_int),
         "lu_status_string": ([ctypes.c_int], ctypes.c_char_p),
+        "lu_profile": ([H, ctypes.c_int], ctypes.c_int),
+        "lu_phase_times": ([H, P, P, P], ctypes.c_int),
+        "lu_launch_count": ([], ctypes.c_int64),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -29,8 +29,12 @@ constexpr int kNumSMsB200 = 148;
     }                                                                           \
   } while (0)
 
+// Count of kernels this library has launched (reported by lu_launch_count).
+extern long long g_kernel_launches;
+
 #define LUB_LAUNCH_CHECK()                                                      \
   do {                                                                          \
+    __atomic_add_fetch(&::lub::g_kernel_launches, 1, __ATOMIC_RELAXED);         \
     cudaError_t _e = cudaGetLastError();                                        \
     if (_e != cudaSuccess) {                                                    \
       fprintf(stderr, "[lu_b200] %s:%d launch -> %s\n", __FILE__, __LINE__,     \

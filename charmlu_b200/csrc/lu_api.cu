@@ -77,6 +77,8 @@ struct MatF64 {
   double* at(int64_t r, int64_t c) const { return p + r * ld + c; }
 };
 
+long long g_kernel_launches = 0;
+
 static int g_init_status = -1000;
 static std::mutex g_init_mu;
 static int ensure_kernels_init() {
@@ -116,6 +118,24 @@ struct lu_handle_s {
   std::vector<void*> allocs;
   size_t bytes = 0;
   long long spin = 0;
+  // phase profiling (events on the launching stream)
+  int profile = 0;
+  struct Rec {
+    int phase;
+    cudaEvent_t a, b;
+    double flops;
+  };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  size_t pool_used = 0;
+  cudaEvent_t take_event() {
+    if (pool_used == pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      pool.push_back(e);
+    }
+    return pool[pool_used++];
+  }
 
   template <typename T>
   int alloc(T** p, size_t count) {
@@ -137,6 +157,28 @@ struct lu_handle_s {
 
 namespace {
 
+// Brackets one phase with events when the handle is profiling.
+struct Prof {
+  lu_handle h;
+  cudaStream_t s;
+  int ph;
+  double fl;
+  cudaEvent_t a = nullptr;
+  Prof(lu_handle h_, cudaStream_t s_, int ph_, double fl_ = 0.0) : h(h_), s(s_), ph(ph_), fl(fl_) {
+    if (h->profile) {
+      a = h->take_event();
+      cudaEventRecord(a, s);
+    }
+  }
+  ~Prof() {
+    if (h->profile) {
+      cudaEvent_t b = h->take_event();
+      cudaEventRecord(b, s);
+      h->recs.push_back({ph, a, b, fl});
+    }
+  }
+};
+
 // even split of a column block, multiple of 16 when wide enough
 inline int split_w(int w) {
   int h = w / 2;
@@ -155,6 +197,7 @@ struct Ctx64 {
 
 int pivots_apply_f64(Ctx64& c, int k0, int cnt, int c_begin, int c_end, int skip_b, int skip_e, double* rhs,
                      int32_t* perm) {
+  Prof pf(c.h, c.s, LU_PH_LASWP);
   for (int off = 0; off < cnt; off += 512) {
     const int sub = std::min(512, cnt - off);
     LUB_TRY(launch_pivot_compose(c.ipiv, k0 + off, sub, c.h->plist, c.s));
@@ -166,7 +209,8 @@ int pivots_apply_f64(Ctx64& c, int k0, int cnt, int c_begin, int c_end, int skip
 
 // C(rc, cc) [M x N] -= A(ra, ca) [M x K] * B(rb, cb) [K x N]
 int gemm64(Ctx64& c, const MatF64& Cm, int rc, int cc, const MatF64& Am, int ra, int ca, const MatF64& Bm, int rb,
-           int cb, int M, int N, int K) {
+           int cb, int M, int N, int K, int phase = LU_PH_GEMM_IN) {
+  Prof pf(c.h, c.s, phase, 2.0 * M * (double)N * K);
   GemmArgs g;
   g.a_row0 = ra; g.a_col0 = ca; g.b_row0 = rb; g.b_col0 = cb;
   g.C = Cm.at(rc, cc); g.ldc = Cm.ld;
@@ -177,7 +221,10 @@ int gemm64(Ctx64& c, const MatF64& Cm, int rc, int cc, const MatF64& Am, int ra,
 
 // B(r0.., cb..) [w x ncols] <- L^{-1} B, L = unit lower of Lm at (r0, r0)
 int trsm64(Ctx64& c, const MatF64& Lm, int r0, int w, const MatF64& Bm, int rb, int cb, int ncols) {
-  if (w <= 32) return launch_trsm_llu_leaf<double>(Lm.at(r0, r0), Lm.ld, Bm.at(rb, cb), Bm.ld, w, ncols, c.s);
+  if (w <= 32) {
+    Prof pf(c.h, c.s, LU_PH_TRSM, (double)w * w * ncols);
+    return launch_trsm_llu_leaf<double>(Lm.at(r0, r0), Lm.ld, Bm.at(rb, cb), Bm.ld, w, ncols, c.s);
+  }
   const int w1 = split_w(w);
   LUB_TRY(trsm64(c, Lm, r0, w1, Bm, rb, cb, ncols));
   LUB_TRY(gemm64(c, Bm, rb + w1, cb, Lm, r0 + w1, r0, Bm, rb, cb, w - w1, ncols, w1));
@@ -190,6 +237,7 @@ int panel64(Ctx64& c, int c0, int w) {
   if (w <= 32) {
     unsigned* bar = c.h->take_counter();
     if (!bar) return LU_ERR_NOMEM;
+    Prof pf(c.h, c.s, LU_PH_PANEL, (double)M * w * w);
     return launch_getf2_leaf<double>(c.A.at(c0, c0), c.A.ld, M, w, c.ipiv + c0, c0, c.h->leaf64, bar, c.h->st, c0,
                                      c.thr, c.h->spin, c.h->num_sms, c.s);
   }
@@ -227,7 +275,7 @@ int factor_f64(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double* rhs,
     const int rest = n - k0 - kw;
     if (rest > 0) {
       LUB_TRY(trsm64(c, c.A, k0, kw, c.A, k0, k0 + kw, rest));
-      LUB_TRY(gemm64(c, c.A, k0 + kw, k0 + kw, c.A, k0 + kw, k0, c.A, k0, k0 + kw, rest, rest, kw));
+      LUB_TRY(gemm64(c, c.A, k0 + kw, k0 + kw, c.A, k0 + kw, k0, c.A, k0, k0 + kw, rest, rest, kw, LU_PH_GEMM));
     }
   }
   return LU_OK;
@@ -236,6 +284,7 @@ int factor_f64(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double* rhs,
 // x <- U^{-1} L^{-1} x (x already permuted)
 int solve_permuted_f64(lu_handle h, const double* LU, int64_t lda, double* x, cudaStream_t s) {
   const int n = (int)h->cfg.n;
+  Prof pf(h, s, LU_PH_SOLVE, 2.0 * n * (double)n);
   LUB_TRY(launch_trsv<double>(LU, lda, n, x, 0, h->trsv_flags, h->trsv_ticket, h->st, h->spin, s));
   LUB_TRY(launch_trsv<double>(LU, lda, n, x, 1, h->trsv_flags, h->trsv_ticket, h->st, h->spin, s));
   return LU_OK;
@@ -325,6 +374,7 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
 
 int lu_destroy(lu_handle h) {
   if (!h) return LU_ERR_ARG;
+  for (cudaEvent_t e : h->pool) cudaEventDestroy(e);
   for (void* p : h->allocs) cudaFree(p);
   if (h->racc_host) cudaFreeHost(h->racc_host);
   delete h;
@@ -432,6 +482,36 @@ int lu_matgen_host(double* out, int64_t count, int32_t seed, int64_t skip) {
   }
   return LU_OK;
 }
+
+int lu_profile(lu_handle h, int enable) {
+  if (!h) return LU_ERR_ARG;
+  h->profile = enable ? 1 : 0;
+  return LU_OK;
+}
+
+int lu_phase_times(lu_handle h, double* ms, int64_t* launches, double* flops) {
+  if (!h) return LU_ERR_ARG;
+  double t[LU_NUM_PHASES] = {0}, f[LU_NUM_PHASES] = {0};
+  int64_t c[LU_NUM_PHASES] = {0};
+  for (auto& r : h->recs) {
+    LUB_CUDA(cudaEventSynchronize(r.b));
+    float e = 0.f;
+    LUB_CUDA(cudaEventElapsedTime(&e, r.a, r.b));
+    t[r.phase] += e;
+    f[r.phase] += r.flops;
+    c[r.phase] += 1;
+  }
+  for (int i = 0; i < LU_NUM_PHASES; i++) {
+    if (ms) ms[i] = t[i];
+    if (launches) launches[i] = c[i];
+    if (flops) flops[i] = f[i];
+  }
+  h->recs.clear();
+  h->pool_used = 0;
+  return LU_OK;
+}
+
+int64_t lu_launch_count(void) { return __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED); }
 
 const char* lu_status_string(int status) {
   if (status > 0) return "singular pivot (info = first failing column, 1-based)";

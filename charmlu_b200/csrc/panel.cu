@@ -207,6 +207,7 @@ int launch_getf2_leaf(T* P, int64_t lda, int M, int ncols, int32_t* ipiv, int ro
   void* args[] = {&P, &lda, &M, &ncols, &R, &ipiv, &row_base, const_cast<LeafScratch<T>*>(&scr), &bar, &st,
                   &info_base, &thr, &spin};
   LUB_CUDA(cudaLaunchCooperativeKernel((const void*)getf2_leaf_kernel<T, W>, dim3(G), dim3(THREADS), args, smem, s));
+  __atomic_add_fetch(&g_kernel_launches, 1, __ATOMIC_RELAXED);
   return LU_OK;
 }
 

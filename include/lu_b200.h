@@ -187,6 +187,26 @@ LU_API int lu_generate_uniform(double* d, int64_t rows, int64_t cols, int64_t ld
  * minimal-standard LCG, seed 9934835 by default.  Host-side. */
 LU_API int lu_matgen_host(double* out, int64_t count, int32_t seed, int64_t skip);
 
+/* Profiling (no reference counterpart; the reference prints per-panel wall
+ * times, lu.ci:282-286, 352-353).  lu_profile(h, 1) makes later calls on h
+ * bracket every phase with CUDA events on the launching stream;
+ * lu_phase_times() synchronises and returns, per phase, the summed device
+ * milliseconds, the launch count and the algorithmic flops of that phase's
+ * launches since the last reset (arrays of LU_NUM_PHASES entries, any may be
+ * NULL), then resets.  Phases: */
+#define LU_PH_PANEL   0  /* leaf getf2 launches */
+#define LU_PH_LASWP   1  /* pivot compose + apply */
+#define LU_PH_TRSM    2  /* TRSM leaves (U block row and panel-internal) */
+#define LU_PH_GEMM    3  /* trailing-update GEMMs (one per panel step) */
+#define LU_PH_GEMM_IN 4  /* GEMM halves inside the recursive panel / TRSM */
+#define LU_PH_SOLVE   5  /* forward / backward substitution */
+#define LU_PH_OTHER   6  /* conversions, residuals, refinement vectors */
+#define LU_NUM_PHASES 7
+LU_API int lu_profile(lu_handle h, int enable);
+LU_API int lu_phase_times(lu_handle h, double* ms, int64_t* launches, double* flops);
+/* Kernels this library has launched since it was loaded (all handles). */
+LU_API int64_t lu_launch_count(void);
+
 /* Message for a status code. */
 LU_API const char* lu_status_string(int status);
 

@@ -13,7 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def _header_symbols():
     txt = open(os.path.join(ROOT, "include", "lu_b200.h")).read()
-    return sorted(set(re.findall(r"^\s*LU_API\s+(?:int|size_t|const char\*)\s+(lu_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^\s*LU_API\s+(?:int|int64_t|size_t|const char\*)\s+(lu_\w+)\s*\(", txt, re.M)))
 
 
 def test_library_loads_and_exports_header_symbols():
