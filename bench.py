@@ -160,6 +160,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=65536)
     ap.add_argument("--block", type=int, default=256)
+    ap.add_argument("--block-mixed", type=int, default=512)
+    ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--mode", default="auto", choices=["auto", "fp64", "mixed"])
     ap.add_argument("--ref-sample", type=int, default=8192)
     ap.add_argument("--no-e2e", action="store_true")
@@ -188,13 +190,17 @@ def main():
         torch.cuda.synchronize()
 
     n, b = args.n, args.block
+    bm = args.block_mixed
     seed = 42 + rank
-    mode = "fp64" if args.mode == "auto" else args.mode
+    mode = "mixed" if args.mode == "auto" else args.mode
     dev = torch.device("cuda", local)
+    peaks = measured_peaks()
 
     A0 = lu.generate_uniform(n, n, seed=seed, stream_id=0, device=dev)
     rhs0 = lu.generate_uniform(n, 1, seed=seed, stream_id=1, device=dev).view(-1)
-    solver = lu.LUSolver(lu.LUConfig(n, b))
+
+    # ---------------- FP64 path: factor_solve on a copy of A0 ----------------
+    s64 = lu.LUSolver(lu.LUConfig(n, b))
     A = torch.empty_like(A0)
     x = torch.empty_like(rhs0)
 
@@ -203,15 +209,30 @@ def main():
         x.copy_(rhs0)
         if ev:
             ev[0].record()
-        solver.factor_solve(A, x)
+        s64.factor_solve(A, x)
         if ev:
             ev[1].record()
 
+    # ---------------- mixed path: refine_solve (A0, b read only) -------------
+    smx = lu.LUSolver(lu.LUConfig(n, bm, precision=lu.LU_PREC_BF16)) if mode == "mixed" else None
+    xm = torch.empty_like(rhs0)
+    last_info = {}
+
+    def step_mixed(ev=None):
+        if ev:
+            ev[0].record()
+        _, inf = smx.refine_solve(A0, rhs0, xm)
+        if ev:
+            ev[1].record()
+        last_info.update(inf)
+
+    headline = step_mixed if mode == "mixed" else step_fp64
+    head_solver = smx if mode == "mixed" else s64
     for _ in range(args.warmup):
-        step_fp64()
-    st = solver.status()
+        headline()
+    st = head_solver.status()
     if st != 0:
-        raise SystemExit(f"warmup status {st}: {lu.status_string(st)}")
+        raise SystemExit(f"warmup status {st}: {lu.status_string(st)} {last_info}")
 
     clocks = ClockSampler(local)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -219,7 +240,7 @@ def main():
     barrier()
     clocks.start()
     for k in range(args.steps):
-        step_fp64(evs[k])
+        headline(evs[k])
     barrier()
     clk = clocks.stop()
     launches = lu.launch_count() - launches0
@@ -229,14 +250,39 @@ def main():
         t = torch.tensor([tot_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         tot_ms = float(t.item())
-    status = solver.status()
-    res = solver.residual(A0, x, rhs0)
+    status = head_solver.status()
+    xh = xm if mode == "mixed" else x
+    res = s64.residual(A0, xh, rhs0)
+    info = dict(last_info)
 
-    # one profiled step (not part of the timed region): per-phase device time
-    solver.profile(True)
-    step_fp64()
-    phases = solver.phase_times()
-    solver.profile(False)
+    # one profiled headline step (outside the timed region)
+    head_solver.profile(True)
+    headline()
+    phases = head_solver.phase_times()
+    head_solver.profile(False)
+
+    # FP64 companion (mixed mode): time-to-solution of the FP64 path, same A, b
+    fp64 = None
+    if mode == "mixed":
+        step_fp64()
+        e = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        fp64_ms = []
+        for _ in range(args.fp64_steps):
+            step_fp64(e)
+            torch.cuda.synchronize()
+            fp64_ms.append(e[0].elapsed_time(e[1]))
+        r64 = s64.residual(A0, x, rhs0)
+        s64.profile(True)
+        step_fp64()
+        ph64 = s64.phase_times()
+        s64.profile(False)
+        fe = ((xm - x).abs().max() / x.abs().max()).item()
+        t64 = sum(fp64_ms) / len(fp64_ms)
+        fp64 = {"time_to_solution_s": t64 / 1e3, "tflops": flops_lu(n) / (t64 / 1e3) / 1e12, "block_size": b,
+                "r_hpl": r64["r_hpl"], "r_ref": r64["r_ref"], "status": s64.status(),
+                "phases_ms": {k: round(v[0], 3) for k, v in ph64.items()},
+                "gemm_tflops": ph64["gemm"][2] / ph64["gemm"][0] / 1e9 if ph64["gemm"][0] else None}
+        info["forward_error_vs_fp64_path"] = fe
 
     # FP64 peak: cuBLAS DGEMM 8192^3 back to back (MEASURED_PEAKS.json has no FP64 entry)
     peak64 = None
@@ -257,35 +303,50 @@ def main():
         del a, bb, c
     except Exception:
         peak64 = None
+    peak64_v = peak64 if peak64 else 35.2
 
     gms, gcalls, gfl = phases["gemm"]
     gemm_tf = gfl / gms / 1e9 if gms > 0 else None
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "gemm_f64_traffic.json")
+    if mode == "mixed":
+        peak_v = peaks.get("bf16_tflops_sustained") or 1376.1
+        roof = {"bound": "tensor", "kernel": "gemm_bf16_tc_kernel (trailing update, tcgen05 kind::f16, TMEM accum)",
+                "achieved": gemm_tf, "peak": peak_v, "unit": "TFLOP/s",
+                "frac": (gemm_tf / peak_v) if gemm_tf else None, "traffic": None,
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"}
+        tpath = os.path.join(ROOT, "profiles", "gemm_bf16_traffic.json")
+    else:
+        roof = {"bound": "tensor", "kernel": "gemm_f64_sub_kernel (trailing update, DMMA)",
+                "achieved": gemm_tf, "peak": peak64_v, "unit": "TFLOP/s",
+                "frac": (gemm_tf / peak64_v) if gemm_tf else None, "traffic": None,
+                "peak_source": "live cuBLAS DGEMM 8192^3 (MEASURED_PEAKS.json has no FP64 entry)"}
+        tpath = os.path.join(ROOT, "profiles", "gemm_f64_traffic.json")
     if os.path.exists(tpath) and gcalls:
         tj = json.load(open(tpath))
-        # captured launch scaled to the average trailing launch by flops
-        traffic = tj["bytes_per_flop"] * gfl / gcalls
+        roof["traffic"] = tj["bytes_per_flop"] * gfl / gcalls
+        roof["traffic_note"] = "bytes per launch, from the ncu capture in " + tj["source"] + " scaled by flops"
 
     line = None
     if rank == 0:
         value = flops_lu(n) * args.steps * world / (tot_ms / 1e3) / 1e12
-        peak_src = "live cuBLAS DGEMM 8192^3 (12 back-to-back)" if peak64 else "fallback 35.2 (cuBLAS DGEMM measured on this pool)"
-        peak_v = peak64 if peak64 else 35.2
         line = {
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16-tensor/f32-panel/f64-ir" if mode == "mixed" else "f64",
             "data": "synthetic uniform[-0.5,0.5) seed 42 (counter-based generator)",
-            "config": {"workload": f"N={n} dense LU with partial pivoting + solve, FP64 path, b={b}",
-                       "n": n, "block_size": b, "path": mode, "l2": "inputs 34 GB >> 126 MB L2 (no flush needed)",
+            "config": {"workload": (f"N={n} dense LU + solve to r_hpl<16: BF16-trailing/FP32-panel factor + FP64 "
+                                    f"refinement (b={bm}), FP64 LU (b={b}) beside it") if mode == "mixed" else
+                       f"N={n} dense LU with partial pivoting + solve, FP64 path, b={b}",
+                       "n": n, "block_size": bm if mode == "mixed" else b, "path": mode,
+                       "l2": "inputs 34 GB >> 126 MB L2 (no flush needed)",
                        "parallelism": "replicas" if world > 1 else "single"},
             "time_to_solution_s": tot_ms / args.steps / 1e3,
             "status": status, "r_hpl": res["r_hpl"], "r_ref": res["r_ref"],
-            "roofline": {"bound": "tensor", "kernel": "gemm_f64_sub (trailing update, DMMA)",
-                         "achieved": gemm_tf, "peak": peak_v, "unit": "TFLOP/s",
-                         "frac": (gemm_tf / peak_v) if gemm_tf else None, "traffic": traffic,
-                         "peak_source": peak_src + "; MEASURED_PEAKS.json has no FP64 entry"},
+            "refine": info if mode == "mixed" else None,
+            "fp64_path": fp64,
+            "speedup_vs_fp64": (fp64["time_to_solution_s"] / (tot_ms / args.steps / 1e3)) if fp64 else None,
+            "roofline": roof,
+            "fp64_peak_tflops": peak64_v,
             "phases_ms": {k: round(v[0], 3) for k, v in phases.items()},
             "gpu_launches": launches,
             "clocks": clk,
@@ -309,10 +370,16 @@ def main():
                 torch.cuda.synchronize()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record()
-                A.copy_(hA, non_blocking=True)
-                x.copy_(hb, non_blocking=True)
-                solver.factor_solve(A, x)
-                hx.copy_(x, non_blocking=True)
+                if mode == "mixed":
+                    A.copy_(hA, non_blocking=True)
+                    x.copy_(hb, non_blocking=True)
+                    smx.refine_solve(A, x, xm)
+                    hx.copy_(xm, non_blocking=True)
+                else:
+                    A.copy_(hA, non_blocking=True)
+                    x.copy_(hb, non_blocking=True)
+                    s64.factor_solve(A, x)
+                    hx.copy_(x, non_blocking=True)
                 e1.record()
                 torch.cuda.synchronize()
                 e2e_ms.append(e0.elapsed_time(e1))

@@ -12,7 +12,7 @@ LIB_PATH = os.path.join(HERE, "liblu_b200.so")
 LU_OK = 0
 LU_ERR_ARG, LU_ERR_CUDA, LU_ERR_TIMEOUT, LU_ERR_NONFINITE = -1, -2, -3, -4
 LU_ERR_NOCONV, LU_ERR_ALIGN, LU_ERR_NOMEM, LU_ERR_UNSUPPORTED = -5, -6, -7, -8
-LU_PREC_FP64, LU_PREC_BF16, LU_PREC_FP16S = 0, 1, 2
+LU_PREC_FP64, LU_PREC_BF16, LU_PREC_FP16S, LU_PREC_FP16X3 = 0, 1, 2, 3
 LU_IR_CLASSIC, LU_IR_GMRES = 0, 1
 
 # every symbol the header declares (checked by the CPU test suite)

@@ -128,6 +128,20 @@ __host__ __device__ __forceinline__ double uniform_at(uint64_t key, uint64_t i) 
   return (double)(z >> 11) * (1.0 / 9007199254740992.0) - 0.5;
 }
 
+// Power-of-two operand scaling for FP16 tensor-core operands: a panel whose
+// largest magnitude is m is multiplied by 2^(13 - floor(log2 m)), which puts
+// its largest entry in [2^13, 2^14) (FP16 max 65504) and keeps the low parts
+// of a hi/lo split in the normal range.  amax holds float bit patterns.
+__host__ __device__ __forceinline__ float pow2_scale_of(float m) {
+  if (!(m > 0.f) || !(m < 3.0e38f)) return 1.f;
+  int e;
+  frexpf(m, &e);  // m = f * 2^e, f in [0.5, 1)  ->  floor(log2 m) = e - 1
+  return ldexpf(1.f, 13 - (e - 1));
+}
+__device__ __forceinline__ float pow2_unscale(const unsigned* amax) {
+  return 1.f / (pow2_scale_of(__uint_as_float(amax[0])) * pow2_scale_of(__uint_as_float(amax[1])));
+}
+
 // ---------------------------------------------------------------------------
 // mbarrier + TMA (cp.async.bulk.tensor) wrappers.  No cluster multicast is
 // used anywhere in this library.

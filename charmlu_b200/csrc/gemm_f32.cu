@@ -1,0 +1,114 @@
+// FP32 C -= A * B (row-major, any M, N, K) for the GEMM halves of the
+// mixed-precision path's recursive FP32 panel and TRSM.  The mixed path keeps
+// its panel and triangular solves in FP32 (only the trailing update drops to
+// BF16 tensor cores), so these run on the FP32 SIMT pipe.
+//
+// Tiling: CTA 128 x 128, K-tile 16, 256 threads with an 8 x 8 register
+// block each (outer products from shared memory); the A tile is stored
+// k-major in shared memory so both operands are read as float4.  Tiles are
+// double-buffered through registers; edges are zero-filled on load.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace lub {
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 16, THREADS = 256;
+
+__global__ void __launch_bounds__(THREADS, 2)
+gemm_f32_sub_kernel(const float* __restrict__ A, int64_t lda, const float* __restrict__ B, int64_t ldb,
+                    float* __restrict__ C, int64_t ldc, int M, int N, int K) {
+  __shared__ __align__(16) float As[2][BK][BM + 4];
+  __shared__ __align__(16) float Bs[2][BK][BN + 4];
+  const int tid = threadIdx.x;
+  const int tm = blockIdx.y * BM, tn = blockIdx.x * BN;
+  const int tx = tid & 15, ty = tid >> 4;  // 16 x 16 threads, 8 x 8 each
+
+  // loader mapping: A tile 128 x 16 -> each thread 8 elements (rows ar, ar+64; k ak..ak+3)
+  const int ar = tid >> 2, ak = (tid & 3) * 4;
+  // B tile 16 x 128 -> each thread 8 elements (k rows bk, bk+8; cols bn..bn+3)
+  const int bk = tid >> 5, bn = (tid & 31) * 4;
+
+  float ra[2][4], rb[2][4];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int r = tm + ar + h * 64;
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int k = k0 + ak + e;
+        ra[h][e] = (r < M && k < K) ? __ldg(&A[(int64_t)r * lda + k]) : 0.f;
+      }
+      const int kb = k0 + bk + h * 8;
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int c = tn + bn + e;
+        rb[h][e] = (kb < K && c < N) ? __ldg(&B[(int64_t)kb * ldb + c]) : 0.f;
+      }
+    }
+  };
+  auto store = [&](int buf) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+#pragma unroll
+      for (int e = 0; e < 4; e++) As[buf][ak + e][ar + h * 64] = ra[h][e];
+      *reinterpret_cast<float4*>(&Bs[buf][bk + h * 8][bn]) = make_float4(rb[h][0], rb[h][1], rb[h][2], rb[h][3]);
+    }
+  };
+
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[i][j] = 0.f;
+
+  const int KT = (K + BK - 1) / BK;
+  load(0);
+  store(0);
+  __syncthreads();
+  for (int kt = 0; kt < KT; kt++) {
+    const int buf = kt & 1;
+    if (kt + 1 < KT) load((kt + 1) * BK);
+#pragma unroll
+    for (int k = 0; k < BK; k++) {
+      const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][k][ty * 4]);
+      const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][k][64 + ty * 4]);
+      const float4 b0 = *reinterpret_cast<const float4*>(&Bs[buf][k][tx * 4]);
+      const float4 b1 = *reinterpret_cast<const float4*>(&Bs[buf][k][64 + tx * 4]);
+      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+    }
+    if (kt + 1 < KT) {
+      store(buf ^ 1);
+      __syncthreads();
+    }
+  }
+  // C -= acc (rows ty*4 + {0..3}, 64 + ty*4 + {0..3}; cols tx*4.., 64 + tx*4..)
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const int r = tm + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+    if (r >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int c = tn + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+      if (c < N) C[(int64_t)r * ldc + c] -= acc[i][j];
+    }
+  }
+}
+
+}  // namespace
+
+int launch_gemm_f32_sub(const float* A, int64_t lda, const float* B, int64_t ldb, float* C, int64_t ldc, int M,
+                        int N, int K, cudaStream_t s) {
+  if (M <= 0 || N <= 0 || K <= 0) return LU_OK;
+  dim3 grid(ceil_div(N, BN), ceil_div(M, BM));
+  gemm_f32_sub_kernel<<<grid, THREADS, 0, s>>>(A, lda, B, ldb, C, ldc, M, N, K);
+  LUB_LAUNCH_CHECK();
+  return LU_OK;
+}
+
+}  // namespace lub

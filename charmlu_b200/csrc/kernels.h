@@ -79,4 +79,32 @@ int launch_gather_perm(const double* b, const int32_t* perm, double* y, int n, c
 int launch_scatter_perm(const double* y, const int32_t* perm, double* b, int n, cudaStream_t s);
 int launch_iota(int32_t* p, int n, cudaStream_t s);
 
+// ---- mixed precision
+int gemm_bf16_init();
+int launch_gemm_bf16_tc(const CUtensorMap& mapA, const CUtensorMap& mapB, const CUtensorMap& mapC, int a_row0,
+                        int b_row0, int c_row0, int c_col0, int M, int N, int K, bool bf16, const unsigned* amax,
+                        DevStatus* st, long long spin, cudaStream_t s);
+// |max| of the L21 (rows x K) and U12 (K x N) FP32 panels into amax[0], amax[1]
+int launch_panel_absmax(const float* L, int64_t ldl, int rows, int K, const float* U, int64_t ldu, int N,
+                        unsigned* amax, cudaStream_t s);
+// low-precision operand panels: nparts K-wide copies, part p is the hi
+// (bit p of lo_mask clear) or lo (set) component of src * scale, scale the
+// power of two of amax[which] (or 1 when amax is null); OUT bf16 or fp16
+template <typename OUT>
+int launch_split_rows(const float* src, int64_t lds, OUT* dst, int64_t ldd, int rows, int K, int nparts,
+                      unsigned lo_mask, const unsigned* amax, int which, cudaStream_t s);
+template <typename OUT>
+int launch_split_transpose(const float* src, int64_t lds, OUT* dst, int64_t ldd, int K, int N, int nparts,
+                           unsigned lo_mask, const unsigned* amax, int which, cudaStream_t s);
+int launch_f64_to_f32(const double* src, int64_t lds, float* dst, int64_t ldd, int rows, int cols, cudaStream_t s);
+int launch_ir_prep(const double* r64, const int32_t* perm, float* r32, int n, const ResidualAccum* acc,
+                   cudaStream_t s);
+int launch_ir_update(double* x, const float* d32, int n, const ResidualAccum* acc, cudaStream_t s);
+int launch_gather_f64_to_f32(const double* v, const int32_t* perm, float* y, int n, double scale, cudaStream_t s);
+int launch_f32_to_f64(const float* y, double* x, int n, double scale, cudaStream_t s);
+// GMRES vector kernels (FP64, basis stored as consecutive length-n vectors)
+int launch_multi_dot(const double* V, int k, const double* w, int n, double* part, double* out, cudaStream_t s);
+int launch_multi_axpy(double* w, const double* V, int k, const double* h, int n, double sign, cudaStream_t s);
+int launch_scale_copy(const double* src, double* dst, int n, const double* inv_of, cudaStream_t s);
+
 }  // namespace lub

@@ -16,8 +16,7 @@
 #include <mutex>
 #include <vector>
 
-#include "common.cuh"
-#include "kernels.h"
+#include "handle.h"
 
 namespace lub {
 
@@ -61,30 +60,15 @@ int encode_tmap_2d(CUtensorMap* map, CUtensorMapDataType dtype, int elem_bytes, 
   return LU_OK;
 }
 
-// A row-major FP64 matrix with the two tensor maps the GEMM reads it by.
-struct MatF64 {
-  double* p = nullptr;
-  int64_t ld = 0, rows = 0, cols = 0;
-  CUtensorMap mapA, mapB;  // boxes 16x128 and 16x16, 128-byte swizzle
-  int init(double* ptr, int64_t r, int64_t c, int64_t ldd) {
-    p = ptr; rows = r; cols = c; ld = ldd;
-    LUB_TRY(encode_tmap_2d(&mapA, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, ptr, c, r, ld * 8, 16, 128,
-                           CU_TENSOR_MAP_SWIZZLE_128B));
-    LUB_TRY(encode_tmap_2d(&mapB, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, ptr, c, r, ld * 8, 16, 16,
-                           CU_TENSOR_MAP_SWIZZLE_128B));
-    return LU_OK;
-  }
-  double* at(int64_t r, int64_t c) const { return p + r * ld + c; }
-};
-
 long long g_kernel_launches = 0;
 
 static int g_init_status = -1000;
 static std::mutex g_init_mu;
-static int ensure_kernels_init() {
+int ensure_kernels_init() {
   std::lock_guard<std::mutex> lk(g_init_mu);
   if (g_init_status != -1000) return g_init_status;
   int s = gemm_f64_init();
+  if (s == LU_OK) s = gemm_bf16_init();
   if (s == LU_OK) s = leaf_init<double>();
   if (s == LU_OK) s = leaf_init<float>();
   g_init_status = s;
@@ -95,89 +79,7 @@ static int ensure_kernels_init() {
 
 using namespace lub;
 
-struct lu_handle_s {
-  lu_config cfg;
-  int device = 0;
-  int num_sms = 148;
-  // workspace (device)
-  DevStatus* st = nullptr;
-  unsigned* counters = nullptr;
-  int n_counters = 0;
-  int next_counter = 0;
-  LeafScratch<double> leaf64{};
-  LeafScratch<float> leaf32{};
-  PivotList plist{};
-  int32_t* perm = nullptr;
-  int32_t* perm_work = nullptr;
-  int* trsv_flags = nullptr;
-  unsigned* trsv_ticket = nullptr;
-  double* vec = nullptr;
-  double* vec2 = nullptr;
-  ResidualAccum* racc = nullptr;
-  ResidualAccum* racc_host = nullptr;
-  std::vector<void*> allocs;
-  size_t bytes = 0;
-  long long spin = 0;
-  // phase profiling (events on the launching stream)
-  int profile = 0;
-  struct Rec {
-    int phase;
-    cudaEvent_t a, b;
-    double flops;
-  };
-  std::vector<Rec> recs;
-  std::vector<cudaEvent_t> pool;
-  size_t pool_used = 0;
-  cudaEvent_t take_event() {
-    if (pool_used == pool.size()) {
-      cudaEvent_t e;
-      cudaEventCreate(&e);
-      pool.push_back(e);
-    }
-    return pool[pool_used++];
-  }
-
-  template <typename T>
-  int alloc(T** p, size_t count) {
-    void* q = nullptr;
-    if (cudaMalloc(&q, std::max<size_t>(count * sizeof(T), 16)) != cudaSuccess) {
-      cudaGetLastError();
-      return LU_ERR_NOMEM;
-    }
-    allocs.push_back(q);
-    bytes += count * sizeof(T);
-    *p = static_cast<T*>(q);
-    return LU_OK;
-  }
-  unsigned* take_counter() {
-    if (next_counter >= n_counters) return nullptr;
-    return counters + next_counter++;
-  }
-};
-
 namespace {
-
-// Brackets one phase with events when the handle is profiling.
-struct Prof {
-  lu_handle h;
-  cudaStream_t s;
-  int ph;
-  double fl;
-  cudaEvent_t a = nullptr;
-  Prof(lu_handle h_, cudaStream_t s_, int ph_, double fl_ = 0.0) : h(h_), s(s_), ph(ph_), fl(fl_) {
-    if (h->profile) {
-      a = h->take_event();
-      cudaEventRecord(a, s);
-    }
-  }
-  ~Prof() {
-    if (h->profile) {
-      cudaEvent_t b = h->take_event();
-      cudaEventRecord(b, s);
-      h->recs.push_back({ph, a, b, fl});
-    }
-  }
-};
 
 // even split of a column block, multiple of 16 when wide enough
 inline int split_w(int w) {
@@ -332,7 +234,7 @@ size_t lu_workspace_bytes(const lu_config* cfg) {
 int lu_create(const lu_config* cfg, lu_handle* out) {
   if (!cfg || !out) return LU_ERR_ARG;
   if (cfg->n <= 0 || cfg->n > (int64_t)1 << 30 || cfg->block_size < 2 || (cfg->block_size & 1)) return LU_ERR_ARG;
-  if (cfg->precision < LU_PREC_FP64 || cfg->precision > LU_PREC_FP16S) return LU_ERR_ARG;
+  if (cfg->precision < LU_PREC_FP64 || cfg->precision > LU_PREC_FP16X3) return LU_ERR_ARG;
   LUB_TRY(ensure_kernels_init());
   lu_handle h = new lu_handle_s();
   h->cfg = *cfg;
@@ -441,12 +343,6 @@ int lu_residual(lu_handle h, const double* dA, int64_t lda, const double* dx, co
   out->r_ref = out->rnorm / ((out->amax * out->xnorm + out->bnorm) * dn * eps);
   out->r_hpl = out->rnorm / ((out->anorm * out->xnorm + out->bnorm) * dn * eps);
   return LU_OK;
-}
-
-int lu_refine_solve(lu_handle h, const double* dA, int64_t lda, const double* db, double* dx, lu_refine_info* info,
-                    void* stream) {
-  (void)h; (void)dA; (void)lda; (void)db; (void)dx; (void)info; (void)stream;
-  return LU_ERR_UNSUPPORTED;
 }
 
 int lu_adjoint(lu_handle h, const double* dLU, int64_t lda, const int32_t* ipiv, const double* dX, int64_t ldx,

@@ -1,0 +1,347 @@
+// Mixed-precision factorisation + FP64 iterative refinement (lu_refine_solve).
+//
+// No reference counterpart (charmlu is FP64 only); the factorisation keeps
+// charmlu's right-looking blocked structure (lu.ci:31-370) with these
+// precisions:
+//   working matrix  FP32 copy of the FP64 A (A itself is never modified)
+//   panel, TRSM     FP32 (leaf getf2 + recursive halves on the FP32 pipe)
+//   trailing update BF16 operands, FP32 accumulation in TMEM (tcgen05),
+//                   subtracted into the FP32 matrix with TMA reduce-add
+//   refinement      FP64 residual r = b - A x against the untouched A, FP32
+//                   correction solve with the low-precision factors, FP64
+//                   update of x; classical IR first, GMRES-IR (left
+//                   preconditioned by the LU factors, FP64 Arnoldi) when the
+//                   classical iteration stops contracting.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "handle.h"
+
+using namespace lub;
+
+namespace {
+
+constexpr int kGmresRestart = 30;
+
+int ensure_mixed(lu_handle h) {
+  if (h->mixed_ready) return LU_OK;
+  const int64_t n = h->cfg.n;
+  const int64_t B = h->cfg.block_size;
+  h->ld32 = (n + 31) & ~int64_t(31);
+  h->nparts = h->cfg.precision == LU_PREC_FP16X3 ? 3 : 1;
+  h->ldk = (h->nparts * B + 63) & ~int64_t(63);
+  h->gm = kGmresRestart;
+  LUB_TRY(h->alloc(&h->A32, (size_t)n * h->ld32));
+  LUB_TRY(h->alloc(&h->Lb, (size_t)n * h->ldk));
+  LUB_TRY(h->alloc(&h->Ub, (size_t)n * h->ldk));
+  LUB_TRY(h->alloc(&h->ipiv32, n));
+  LUB_TRY(h->alloc(&h->amax, 4));
+  LUB_TRY(h->alloc(&h->v32, n));
+  LUB_TRY(h->alloc(&h->r64, n));
+  LUB_TRY(h->alloc(&h->z64, n));
+  LUB_TRY(h->alloc(&h->zero64, n));
+  LUB_TRY(h->alloc(&h->V, (size_t)(h->gm + 1) * n));
+  LUB_TRY(h->alloc(&h->hdot, 128 * 64 + 64));
+  LUB_CUDA(cudaMemset(h->zero64, 0, sizeof(double) * n));
+  h->mixed_ready = true;
+  return LU_OK;
+}
+
+struct Ctx32 {
+  lu_handle h;
+  float* A;
+  int64_t ld;
+  int n;
+  int32_t* ipiv;
+  cudaStream_t s;
+  double thr;
+};
+
+inline int split_w32(int w) {
+  int hh = w / 2;
+  int w1 = hh >= 16 ? (hh & ~15) : (hh & ~3);
+  return std::max(w1, 4);
+}
+
+int pivots_apply_f32(Ctx32& c, int k0, int cnt, int c_begin, int c_end, int skip_b, int skip_e, int32_t* perm) {
+  Prof pf(c.h, c.s, LU_PH_LASWP);
+  for (int off = 0; off < cnt; off += 512) {
+    const int sub = std::min(512, cnt - off);
+    LUB_TRY(launch_pivot_compose(c.ipiv, k0 + off, sub, c.h->plist, c.s));
+    LUB_TRY(launch_pivot_apply<float>(c.A, c.ld, c_begin, c_end, skip_b, skip_e, c.h->plist, 2 * sub, nullptr, perm,
+                                      c.s));
+  }
+  return LU_OK;
+}
+
+int sgemm(Ctx32& c, int rc, int cc, int ra, int ca, int rb, int cb, int M, int N, int K) {
+  Prof pf(c.h, c.s, LU_PH_GEMM_IN, 2.0 * M * (double)N * K);
+  return launch_gemm_f32_sub(c.A + (int64_t)ra * c.ld + ca, c.ld, c.A + (int64_t)rb * c.ld + cb, c.ld,
+                             c.A + (int64_t)rc * c.ld + cc, c.ld, M, N, K, c.s);
+}
+
+int trsm32(Ctx32& c, int r0, int w, int rb, int cb, int ncols) {
+  if (w <= 32) {
+    Prof pf(c.h, c.s, LU_PH_TRSM, (double)w * w * ncols);
+    return launch_trsm_llu_leaf<float>(c.A + (int64_t)r0 * c.ld + r0, c.ld, c.A + (int64_t)rb * c.ld + cb, c.ld, w,
+                                       ncols, c.s);
+  }
+  const int w1 = split_w32(w);
+  LUB_TRY(trsm32(c, r0, w1, rb, cb, ncols));
+  LUB_TRY(sgemm(c, rb + w1, cb, r0 + w1, r0, rb, cb, w - w1, ncols, w1));
+  return trsm32(c, r0 + w1, w - w1, rb + w1, cb, ncols);
+}
+
+int panel32(Ctx32& c, int c0, int w) {
+  const int M = c.n - c0;
+  if (w <= 64) {
+    unsigned* bar = c.h->take_counter();
+    if (!bar) return LU_ERR_NOMEM;
+    Prof pf(c.h, c.s, LU_PH_PANEL, (double)M * w * w);
+    return launch_getf2_leaf<float>(c.A + (int64_t)c0 * c.ld + c0, c.ld, M, w, c.ipiv + c0, c0, c.h->leaf32, bar,
+                                    c.h->st, c0, c.thr, c.h->spin, c.h->num_sms, c.s);
+  }
+  const int w1 = split_w32(w), w2 = w - w1;
+  LUB_TRY(panel32(c, c0, w1));
+  LUB_TRY(pivots_apply_f32(c, c0, w1, c0 + w1, c0 + w, 0, 0, nullptr));
+  LUB_TRY(trsm32(c, c0, w1, c0, c0 + w1, w2));
+  LUB_TRY(sgemm(c, c0 + w1, c0 + w1, c0 + w1, c0, c0, c0 + w1, M - w1, w2, w1));
+  LUB_TRY(panel32(c, c0 + w1, w2));
+  return pivots_apply_f32(c, c0 + w1, w2, c0, c0 + w1, 0, 0, nullptr);
+}
+
+// LU of h->A32 in place: FP32 panels/TRSM, BF16 tcgen05 trailing updates.
+int factor_mixed(lu_handle h, cudaStream_t s) {
+  const int n = (int)h->cfg.n, B = h->cfg.block_size;
+  const bool bf16 = h->cfg.precision == LU_PREC_BF16;
+  Ctx32 c{h, h->A32, h->ld32, n, h->ipiv32, s, h->cfg.sing_threshold};
+  CUtensorMap mapC;
+  LUB_TRY(encode_tmap_2d(&mapC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->A32, n, n, h->ld32 * 4, 32, 128,
+                         CU_TENSOR_MAP_SWIZZLE_128B));
+  LUB_CUDA(cudaMemsetAsync(h->counters, 0, sizeof(unsigned) * h->n_counters, s));
+  h->next_counter = 0;
+  LUB_TRY(launch_iota(h->perm, n, s));
+  for (int k0 = 0; k0 < n; k0 += B) {
+    const int kw = std::min(B, n - k0);
+    LUB_TRY(panel32(c, k0, kw));
+    LUB_TRY(pivots_apply_f32(c, k0, kw, 0, n, k0, k0 + kw, h->perm));
+    const int k1 = k0 + kw, rest = n - k1;
+    if (rest <= 0) continue;
+    LUB_TRY(trsm32(c, k0, kw, k0, k1, rest));
+    const float* L21 = c.A + (int64_t)k1 * c.ld + k0;
+    const float* U12 = c.A + (int64_t)k0 * c.ld + k1;
+    const int ke = h->nparts * kw;  // K of the low-precision product (3 K-blocks for the split)
+    {
+      Prof pf(h, s, LU_PH_OTHER);
+      if (bf16) {
+        LUB_TRY(launch_split_rows<__nv_bfloat16>(L21, c.ld, h->Lb, h->ldk, rest, kw, 1, 0u, nullptr, 0, s));
+        LUB_TRY(launch_split_transpose<__nv_bfloat16>(U12, c.ld, h->Ub, h->ldk, kw, rest, 1, 0u, nullptr, 1, s));
+      } else {
+        // L parts [hi, hi, lo] against U parts [hi, lo, hi]: Lh*Uh + Lh*Ul + Ll*Uh
+        LUB_TRY(launch_panel_absmax(L21, c.ld, rest, kw, U12, c.ld, rest, h->amax, s));
+        LUB_TRY(launch_split_rows<__half>(L21, c.ld, reinterpret_cast<__half*>(h->Lb), h->ldk, rest, kw, h->nparts,
+                                          0x4u, h->amax, 0, s));
+        LUB_TRY(launch_split_transpose<__half>(U12, c.ld, reinterpret_cast<__half*>(h->Ub), h->ldk, kw, rest,
+                                               h->nparts, 0x2u, h->amax, 1, s));
+      }
+    }
+    const CUtensorMapDataType dt = bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    CUtensorMap mapL, mapU;
+    LUB_TRY(encode_tmap_2d(&mapL, dt, 2, h->Lb, ke, rest, h->ldk * 2, 64, 128, CU_TENSOR_MAP_SWIZZLE_128B));
+    LUB_TRY(encode_tmap_2d(&mapU, dt, 2, h->Ub, ke, rest, h->ldk * 2, 64, 256, CU_TENSOR_MAP_SWIZZLE_128B));
+    Prof pf(h, s, LU_PH_GEMM, 2.0 * rest * (double)rest * ke);
+    LUB_TRY(launch_gemm_bf16_tc(mapL, mapU, mapC, 0, 0, k1, k1, rest, rest, ke, bf16, bf16 ? nullptr : h->amax,
+                                h->st, h->spin, s));
+  }
+  return LU_OK;
+}
+
+int solve32(lu_handle h, float* v, cudaStream_t s) {
+  const int n = (int)h->cfg.n;
+  Prof pf(h, s, LU_PH_SOLVE, 2.0 * n * (double)n);
+  LUB_TRY(launch_trsv<float>(h->A32, h->ld32, n, v, 0, h->trsv_flags, h->trsv_ticket, h->st, h->spin, s));
+  return launch_trsv<float>(h->A32, h->ld32, n, v, 1, h->trsv_flags, h->trsv_ticket, h->st, h->spin, s);
+}
+
+double bits_to_double(unsigned long long v) {
+  double x;
+  memcpy(&x, &v, 8);
+  return x;
+}
+
+// r = b - A x, its norms, and r_hpl (synchronises).
+int residual_hpl(lu_handle h, const double* A, int64_t lda, const double* x, const double* b, double* r,
+                 double* r_hpl, double* rnorm, cudaStream_t s) {
+  const int n = (int)h->cfg.n;
+  {
+    Prof pf(h, s, LU_PH_OTHER);
+    LUB_TRY(launch_residual_f64(A, lda, n, x, b, r, h->racc, s));
+  }
+  LUB_CUDA(cudaMemcpyAsync(h->racc_host, h->racc, sizeof(ResidualAccum), cudaMemcpyDeviceToHost, s));
+  LUB_CUDA(cudaStreamSynchronize(s));
+  const ResidualAccum& a = *h->racc_host;
+  const double eps = 2.220446049250313e-16;
+  const double an = bits_to_double(a.anorm), xn = bits_to_double(a.xmax), bn = bits_to_double(a.bmax),
+               rn = bits_to_double(a.rmax);
+  *rnorm = rn;
+  *r_hpl = rn / ((an * xn + bn) * (double)n * eps);
+  return LU_OK;
+}
+
+int device_status(lu_handle h, cudaStream_t s) {
+  DevStatus st;
+  LUB_CUDA(cudaMemcpyAsync(&st, h->st, sizeof(st), cudaMemcpyDeviceToHost, s));
+  LUB_CUDA(cudaStreamSynchronize(s));
+  return st.code != 0 ? st.code : st.info;
+}
+
+// Right-preconditioned-equivalent left-preconditioned GMRES on the
+// correction: M^{-1} A d = M^{-1} r with M = P^T L U (FP32 factors), FP64
+// Arnoldi with two passes of classical Gram-Schmidt.  x += d.
+// rnorm: ||r||inf of the residual in h->r64 (the start vector is built from
+// r / rnorm, so the Krylov right-hand side is beta * rnorm).
+int gmres_correction(lu_handle h, const double* A, int64_t lda, double* x, double rnorm, cudaStream_t s,
+                     int* iters_out) {
+  const int n = (int)h->cfg.n, m = h->gm;
+  double* V = h->V;
+  double* part = h->hdot;
+  double* hd = h->hdot + 128 * 64;  // 64 doubles of results
+  std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1, 0.0), hcol(m + 1);
+  // v0 = M^{-1} r / ||M^{-1} r||  (r already in h->r64, racc holds ||r||)
+  LUB_TRY(launch_ir_prep(h->r64, h->perm, h->v32, n, h->racc, s));
+  LUB_TRY(solve32(h, h->v32, s));
+  LUB_TRY(launch_f32_to_f64(h->v32, V, n, 1.0, s));
+  LUB_TRY(launch_multi_dot(V, 1, V, n, part, hd, s));
+  double beta2 = 0.0;
+  LUB_CUDA(cudaMemcpyAsync(&beta2, hd, sizeof(double), cudaMemcpyDeviceToHost, s));
+  LUB_CUDA(cudaStreamSynchronize(s));
+  const double beta = std::sqrt(beta2);
+  if (!(beta > 0.0) || !std::isfinite(beta)) return LU_ERR_NONFINITE;
+  LUB_TRY(launch_scale_copy(V, V, n, hd, s));
+  g[0] = beta * rnorm;
+  int k = 0;
+  for (int j = 0; j < m; j++) {
+    double* vj = V + (size_t)j * n;
+    double* w = V + (size_t)(j + 1) * n;
+    // w = M^{-1} A v_j   (residual kernel with b = 0 gives -A v_j)
+    {
+      Prof pf(h, s, LU_PH_OTHER);
+      LUB_TRY(launch_residual_f64(A, lda, n, vj, h->zero64, h->z64, h->racc, s));
+    }
+    LUB_TRY(launch_gather_f64_to_f32(h->z64, h->perm, h->v32, n, -1.0, s));
+    LUB_TRY(solve32(h, h->v32, s));
+    LUB_TRY(launch_f32_to_f64(h->v32, w, n, 1.0, s));
+    // two passes of classical Gram-Schmidt
+    std::fill(hcol.begin(), hcol.end(), 0.0);
+    for (int pass = 0; pass < 2; pass++) {
+      LUB_TRY(launch_multi_dot(V, j + 1, w, n, part, hd, s));
+      LUB_TRY(launch_multi_axpy(w, V, j + 1, hd, n, -1.0, s));
+      std::vector<double> tmp(j + 1);
+      LUB_CUDA(cudaMemcpyAsync(tmp.data(), hd, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, s));
+      LUB_CUDA(cudaStreamSynchronize(s));
+      for (int i = 0; i <= j; i++) hcol[i] += tmp[i];
+    }
+    LUB_TRY(launch_multi_dot(w, 1, w, n, part, hd, s));
+    double hn2 = 0.0;
+    LUB_CUDA(cudaMemcpyAsync(&hn2, hd, sizeof(double), cudaMemcpyDeviceToHost, s));
+    LUB_CUDA(cudaStreamSynchronize(s));
+    hcol[j + 1] = std::sqrt(hn2);
+    if (hcol[j + 1] > 0.0) LUB_TRY(launch_scale_copy(w, w, n, hd, s));
+    // Givens rotations
+    for (int i = 0; i < j; i++) {
+      const double t = cs[i] * hcol[i] + sn[i] * hcol[i + 1];
+      hcol[i + 1] = -sn[i] * hcol[i] + cs[i] * hcol[i + 1];
+      hcol[i] = t;
+    }
+    const double den = std::hypot(hcol[j], hcol[j + 1]);
+    cs[j] = den > 0 ? hcol[j] / den : 1.0;
+    sn[j] = den > 0 ? hcol[j + 1] / den : 0.0;
+    hcol[j] = den;
+    hcol[j + 1] = 0.0;
+    g[j + 1] = -sn[j] * g[j];
+    g[j] = cs[j] * g[j];
+    for (int i = 0; i <= j; i++) H[(size_t)i * m + j] = hcol[i];
+    k = j + 1;
+    if (std::fabs(g[j + 1]) <= 1e-10 * beta * rnorm) break;
+  }
+  // y = H(1:k,1:k)^{-1} g(1:k); d = V y ; x += d
+  std::vector<double> y(k, 0.0);
+  for (int i = k - 1; i >= 0; i--) {
+    double t = g[i];
+    for (int q = i + 1; q < k; q++) t -= H[(size_t)i * m + q] * y[q];
+    y[i] = t / H[(size_t)i * m + i];
+  }
+  LUB_CUDA(cudaMemcpyAsync(hd, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
+  LUB_TRY(launch_multi_axpy(x, V, k, hd, n, 1.0, s));
+  LUB_CUDA(cudaStreamSynchronize(s));
+  *iters_out = k;
+  return LU_OK;
+}
+
+int refine_solve(lu_handle h, const double* A, int64_t lda, const double* b, double* x, lu_refine_info* info,
+                 cudaStream_t s) {
+  const int n = (int)h->cfg.n;
+  LUB_TRY(ensure_mixed(h));
+  LUB_CUDA(cudaMemsetAsync(h->st, 0, sizeof(DevStatus), s));
+  {
+    Prof pf(h, s, LU_PH_OTHER);
+    LUB_TRY(launch_f64_to_f32(A, lda, h->A32, h->ld32, n, n, s));
+  }
+  LUB_TRY(factor_mixed(h, s));
+  // x0 = U^{-1} L^{-1} P b in FP32
+  LUB_TRY(launch_gather_f64_to_f32(b, h->perm, h->v32, n, 1.0, s));
+  LUB_TRY(solve32(h, h->v32, s));
+  LUB_TRY(launch_f32_to_f64(h->v32, x, n, 1.0, s));
+  const int fst = device_status(h, s);
+  lu_refine_info ri;
+  memset(&ri, 0, sizeof(ri));
+  if (fst != LU_OK) {
+    ri.status = fst;
+    if (info) *info = ri;
+    return LU_OK;  // numerical status is reported through lu_status / info
+  }
+  const double target = h->cfg.ir_target > 0 ? h->cfg.ir_target : 16.0;
+  const int max_it = h->cfg.ir_max_iter > 0 ? h->cfg.ir_max_iter : 50;
+  bool gm = h->cfg.ir_mode == LU_IR_GMRES;
+  double prev = INFINITY, r_hpl = INFINITY, rn = 0.0;
+  int it = 0;
+  for (; it < max_it; it++) {
+    LUB_TRY(residual_hpl(h, A, lda, x, b, h->r64, &r_hpl, &rn, s));
+    if (it == 0) ri.r_hpl_initial = r_hpl;
+    if (!std::isfinite(r_hpl)) break;
+    if (r_hpl < target) break;
+    if (!gm && it >= 2 && r_hpl > 0.5 * prev) gm = true;  // classical IR stopped contracting
+    prev = r_hpl;
+    if (gm) {
+      int k = 0;
+      LUB_TRY(gmres_correction(h, A, lda, x, rn, s, &k));
+      ri.used_gmres = 1;
+      ri.gmres_iterations += k;
+    } else {
+      LUB_TRY(launch_ir_prep(h->r64, h->perm, h->v32, n, h->racc, s));
+      LUB_TRY(solve32(h, h->v32, s));
+      LUB_TRY(launch_ir_update(x, h->v32, n, h->racc, s));
+      ri.iterations++;
+    }
+  }
+  ri.r_hpl = r_hpl;
+  ri.status = (std::isfinite(r_hpl) && r_hpl < target) ? LU_OK : LU_ERR_NOCONV;
+  if (ri.status != LU_OK) {
+    int code = ri.status;
+    LUB_CUDA(cudaMemcpyAsync(&h->st->code, &code, sizeof(int), cudaMemcpyHostToDevice, s));
+  }
+  if (info) *info = ri;
+  return LU_OK;
+}
+
+}  // namespace
+
+extern "C" int lu_refine_solve(lu_handle h, const double* dA, int64_t lda, const double* db, double* dx,
+                               lu_refine_info* info, void* stream) {
+  if (!h || !dA || !db || !dx || lda < h->cfg.n) return LU_ERR_ARG;
+  if (h->cfg.precision == LU_PREC_FP64) return LU_ERR_UNSUPPORTED;
+  if (h->cfg.block_size % 64) return LU_ERR_ARG;  // whole 64-wide BF16 k-blocks per panel
+  LUB_TRY(ensure_kernels_init());
+  return refine_solve(h, dA, lda, db, dx, info, (cudaStream_t)stream);
+}

@@ -60,7 +60,9 @@ extern "C" {
 /* ---- precision of the factorisation ---------------------------------- */
 #define LU_PREC_FP64   0   /* the reference's arithmetic (all FP64) */
 #define LU_PREC_BF16   1   /* FP32 panel/TRSM, BF16 tensor-core trailing update, FP64 refinement */
-#define LU_PREC_FP16S  2   /* as BF16 but FP16 operands with per-tile scaling */
+#define LU_PREC_FP16S  2   /* as BF16 but FP16 operands with per-panel power-of-two scaling */
+#define LU_PREC_FP16X3 3   /* error-compensated FP16: each FP32 operand split hi + lo (scaled FP16), the
+                              update sums Lh*Uh + Lh*Ul + Ll*Uh on the tensor cores (near-FP32 factors) */
 
 /* ---- refinement mode --------------------------------------------------- */
 #define LU_IR_CLASSIC  0   /* classical iterative refinement, GMRES-IR fallback on stagnation */

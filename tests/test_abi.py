@@ -27,6 +27,9 @@ def test_library_loads_and_exports_header_symbols():
     out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
     exported = set(re.findall(r" T (lu_\w+)$", out, re.M))
     assert exported == set(syms), exported ^ set(syms)
+    # the only other exports are unit-test hooks of internal kernels
+    others = set(re.findall(r" T (\w+)$", out, re.M)) - exported
+    assert all(o.startswith("lub_test_") for o in others), others
 
 
 def test_status_strings_and_config_defaults():

@@ -1,0 +1,136 @@
+"""GPU tests of the mixed-precision path (no reference counterpart: charmlu is
+FP64 only).  The BF16 tensor-core kernel is checked against a plain FP64
+torch product of the same BF16-rounded operands; the refined solutions
+against the oracle's FP64 solution (forward error) and the scaled residual
+contract r_hpl < 16."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _lib():
+    from charmlu_b200 import _lib as L
+    lib = L.load()
+    f = lib.lub_test_gemm_lowp
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                  ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    f.restype = ctypes.c_int
+    return f
+
+
+def _pow2_scale(t):
+    m = t.abs().max().item()
+    e = np.frexp(m)[1]  # m = f * 2^e, f in [0.5, 1)
+    return 2.0 ** (13 - (e - 1))
+
+
+def _lowp_reference(A, B, C, mode):
+    """C - product, the product formed exactly (FP64) from the operands the
+    kernel sees: BF16-rounded (mode 0), FP16 of the power-of-two scaled
+    panel (mode 1), or the hi/lo FP16 split with three products (mode 2)."""
+    if mode == 0:
+        return C.double() - A.bfloat16().double() @ B.bfloat16().double()
+    sa, sb = _pow2_scale(A), _pow2_scale(B)
+    As, Bs = A * sa, B * sb
+    Ah, Bh = As.half(), Bs.half()
+    if mode == 1:
+        P = Ah.double() @ Bh.double()
+    else:
+        Al = (As - Ah.float()).half()
+        Bl = (Bs - Bh.float()).half()
+        P = Ah.double() @ Bh.double() + Ah.double() @ Bl.double() + Al.double() @ Bh.double()
+    return C.double() - P / (sa * sb)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("M,N,K", [(128, 256, 64), (300, 520, 256), (1024, 1024, 512), (257, 999, 1024),
+                                   (4096, 4096, 256)])
+def test_gemm_lowp_tcgen05_matches_reference(cuda_dev, M, N, K, mode):
+    f = _lib()
+    g = torch.Generator(device="cuda").manual_seed(M * 7 + N)
+    A = torch.rand(M, K, device="cuda", generator=g, dtype=torch.float32) - 0.5
+    B = (torch.rand(K, N, device="cuda", generator=g, dtype=torch.float32) - 0.5) * 37.0
+    ldc = (N + 3) // 4 * 4
+    Cbuf = torch.rand(M, ldc, device="cuda", generator=g, dtype=torch.float32) - 0.5
+    C = Cbuf[:, :N]
+    pad_before = Cbuf[:, N:].clone()
+    ref = _lowp_reference(A, B, C, mode)
+    rc = f(A.data_ptr(), K, B.data_ptr(), N, Cbuf.data_ptr(), ldc, M, N, K, mode,
+           torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert rc == 0
+    err = (C.double() - ref).abs().max().item()
+    # FP32 accumulation of K (3K for the split) products |a b| <= 0.5 * 18.5:
+    # a statistical bound 4 u32 K max|a b| (the worst-case bound is K^2 u32 max|ab|)
+    kk = K * (3 if mode == 2 else 1)
+    assert err <= 4 * 6e-8 * kk * 0.5 * 18.5 + 1e-6, err
+    assert torch.equal(Cbuf[:, N:], pad_before)
+    if mode == 2:
+        # the three-product split reproduces the exact FP32 product to ~u_fp16^2
+        split = -_lowp_reference(A, B, torch.zeros_like(C), 2)
+        assert (split - A.double() @ B.double()).abs().max().item() <= 1e-5 * 18.5 * K / 64
+
+
+def _refine(n, b, A_np=None, seed=42, mode=None, target=16.0, prec=None):
+    import charmlu_b200 as lu
+    prec = lu.LU_PREC_FP16X3 if prec is None else prec
+    if A_np is None:
+        A = lu.generate_uniform(n, n, seed=seed, stream_id=0)
+    else:
+        A = torch.from_numpy(A_np).cuda()
+    rhs = lu.generate_uniform(n, 1, seed=seed, stream_id=1).view(-1)
+    cfg = lu.LUConfig(n, b, precision=prec, ir_target=target)
+    if mode is not None:
+        cfg.ir_mode = mode
+    s = lu.LUSolver(cfg)
+    x, info = s.refine_solve(A, rhs)
+    st = s.status()
+    return s, A, rhs, x, info, st
+
+
+@pytest.mark.parametrize("prec,n,b", [(1, 512, 256), (2, 512, 256), (2, 1024, 256), (3, 1024, 256), (3, 2048, 512),
+                                      (3, 3000, 256), (3, 4096, 512)])
+def test_refine_solve_reaches_residual_target(cuda_dev, prec, n, b):
+    s, A, rhs, x, info, st = _refine(n, b, prec=prec)
+    assert st == 0 and info["status"] == 0, info
+    r = s.residual(A, x, rhs)
+    assert r["r_hpl"] < 16, r
+    # forward error against the FP64 oracle solution
+    x_ref, *_ = oracle.solve(A.cpu().numpy(), rhs.cpu().numpy(), b=128)
+    fe = np.abs(x.cpu().numpy() - x_ref).max() / np.abs(x_ref).max()
+    assert fe < 1e-6, fe
+    # the low-precision solve alone is far from the target; refinement did the work
+    assert info["r_hpl_initial"] > info["r_hpl"]
+
+
+def test_refine_tight_target_matches_fp64(cuda_dev):
+    """Refined to r_hpl < 0.01 the mixed solution agrees with the FP64 one."""
+    n, b = 2048, 256
+    s, A, rhs, x, info, st = _refine(n, b, target=0.01)
+    assert st == 0 and info["status"] == 0, info
+    x_ref, *_ = oracle.solve(A.cpu().numpy(), rhs.cpu().numpy(), b=128)
+    fe = np.abs(x.cpu().numpy() - x_ref).max() / np.abs(x_ref).max()
+    assert fe < 1e-10, fe
+
+
+def test_gmres_ir_mode(cuda_dev):
+    import charmlu_b200 as lu
+    n, b = 1024, 256
+    s, A, rhs, x, info, st = _refine(n, b, mode=lu.LU_IR_GMRES)
+    assert st == 0 and info["status"] == 0 and info["used_gmres"] == 1, info
+    assert s.residual(A, x, rhs)["r_hpl"] < 16
+
+
+def test_singular_matrix_reports_info_mixed(cuda_dev):
+    import charmlu_b200 as lu
+    n, b = 256, 64
+    A = oracle.gen_matrix(n, 3)
+    A[:, 100] = 0.0
+    s, Ad, rhs, x, info, st = _refine(n, b, A_np=A)
+    assert st == 101, (st, info)
