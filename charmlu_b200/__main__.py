@@ -1,0 +1,87 @@
+"""Command-line drop-in for charmlu's driver.
+
+    python -m charmlu_b200 <matrix size> <block size> <mem threshold>
+                           [<pivot batch size> <mapping scheme> [<peTileRows> <peTileCols> <peRotate> <peStride>]]
+                           [--precision fp64|bf16|fp16s|fp16x3] [--seed S] [--json]
+
+Same positional arguments as charmlu (benchmark.C:81-134); the memory
+threshold, mapping scheme and PE-tile arguments configure Charm++ placement
+and are accepted and ignored on one GPU.  Prints the reference's result
+lines (benchmark.C:151-184, 352-356, 394-395), including the
+``residual = %f`` line that test_lu.pl parses (test_lu.pl:76-77).  A is the
+counter-based uniform[-0.5,0.5) matrix; b is the reference's MatGen stream
+(seed 9934835, benchmark.C:455-460).
+"""
+import argparse
+import json
+import sys
+import time
+
+
+def main(argv=None):
+    argv = sys.argv[1:] if argv is None else argv
+    ap = argparse.ArgumentParser(prog="charmlu_b200", add_help=True)
+    ap.add_argument("positional", nargs="*", type=int)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "bf16", "fp16s", "fp16x3"])
+    ap.add_argument("--seed", type=int, default=42)
+    ap.add_argument("--json", action="store_true")
+    a = ap.parse_args(argv)
+    if len(a.positional) < 3:
+        print("Usage: charmlu_b200 <matrix size> <block size> <mem threshold> [<pivot batch size> <mapping scheme>"
+              " [<peTileRows> <peTileCols> <peRotate> <peStride>] ]")
+        return 0
+    n, b, mem = a.positional[:3]
+    batch = a.positional[3] if len(a.positional) >= 4 else b // 4
+    mapping = a.positional[4] if len(a.positional) >= 5 else 2
+    if b <= 0 or n <= 0:
+        print(f"The matrix size {n} should be a multiple of block size {b}!")
+        return 0
+    if n % b != 0:
+        # the reference refuses (benchmark.C:143-147); the same check is kept for drop-in behaviour
+        print(f"The matrix size {n} should be a multiple of block size {b}!")
+        return 0
+
+    import torch
+    import charmlu_b200 as lu
+    prec = {"fp64": lu.LU_PREC_FP64, "bf16": lu.LU_PREC_BF16, "fp16s": lu.LU_PREC_FP16S,
+            "fp16x3": lu.LU_PREC_FP16X3}[a.precision]
+    print("Running LU compiled from revision: charmlu_b200")
+    print(f"Running LU on 1 processors (1 nodes): \n\tMatrix size: {n} X {n} \n\tBlock size: {b} X {b} "
+          f"\n\tChare Array size: {n // b} X {n // b}\n\tPivot batch size: {batch}\n\tMem Threshold (MB): {mem}"
+          f"\n\tSend Limit: 0\n\tMapping Scheme: {mapping} ({'Block Cyclic' if mapping == 2 else '2D Tiling'})")
+    A = lu.generate_uniform(n, n, seed=a.seed, stream_id=0)
+    bvec = torch.from_numpy(lu.matgen(n)).cuda()
+    A0 = A.clone()
+    x = bvec.clone()
+    blk = b if prec == lu.LU_PREC_FP64 or b % 64 == 0 else 64 * max(1, b // 64)
+    s = lu.LUSolver(lu.LUConfig(n, blk, pivot_batch_size=batch, mem_threshold=mem, precision=prec))
+    print("Starting solve")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    info = None
+    if prec == lu.LU_PREC_FP64:
+        s.factor_solve(A, x)
+    else:
+        x, info = s.refine_solve(A0, bvec)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    st = s.status()
+    if st > 0:
+        print("Diagonal element very small despite pivoting. Is the matrix singular??")
+    gflops = (2.0 / 3.0 * n ** 3 + 1.5 * n ** 2) / dt / 1e9
+    print(f"RESULT procs: \t1\tblock size:\t{b}\tTime(s):\t{dt}")
+    print(f"HPL flop count gives \t{gflops}\tGFlops")
+    r = s.residual(A0, x, bvec)
+    print(f"epsilon = {lu.EPS:e}\nresidual = {r['r_ref']:f}")
+    if r["r_ref"] > 16:
+        print("=== WARNING: Scaled residual is greater than 16 - OUT OF SPEC ===")
+    print(f"r_hpl = {r['r_hpl']:f}")
+    if a.json:
+        print(json.dumps({"n": n, "b": b, "precision": a.precision, "time_s": dt, "gflops_ref_count": gflops,
+                          "tflops": (2 / 3 * n ** 3 + 2 * n ** 2) / dt / 1e12, "status": st, "refine": info, **r}))
+    print("Finished solve")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
