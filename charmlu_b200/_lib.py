@@ -20,7 +20,7 @@ EXPORTS = [
     "lu_config_default", "lu_create", "lu_destroy", "lu_workspace_bytes", "lu_status", "lu_factor",
     "lu_solve", "lu_factor_solve", "lu_residual", "lu_refine_solve", "lu_adjoint",
     "lu_batched_factor_solve", "lu_generate_uniform", "lu_matgen_host", "lu_status_string",
-    "lu_profile", "lu_phase_times", "lu_launch_count",
+    "lu_profile", "lu_phase_times", "lu_launch_count", "lu_solve_noalloc",
 ]
 PHASES = ["panel", "laswp", "trsm", "gemm", "gemm_inner", "solve", "other"]
 
@@ -76,6 +76,7 @@ def load():
         "lu_profile": ([H, ctypes.c_int], ctypes.c_int),
         "lu_phase_times": ([H, P, P, P], ctypes.c_int),
         "lu_launch_count": ([], ctypes.c_int64),
+        "lu_solve_noalloc": ([P, i64, i64, P, P, P, P], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -55,6 +55,8 @@ int launch_pivot_compose(const int32_t* ipiv, int k0, int cnt, const PivotList& 
 template <typename T>
 int launch_pivot_apply(T* A, int64_t lda, int c_begin, int c_end, int skip_begin, int skip_end, const PivotList& pl,
                        int max_m, double* rhs, int32_t* perm, cudaStream_t s);
+// x <- P x in place from an ipiv vector (single CTA, shared memory only).
+int launch_ipiv_apply_vector(const int32_t* ipiv, int n, double* x, cudaStream_t s);
 // Full permutation from an ipiv vector (single CTA, batched composition).
 int launch_ipiv_to_perm(const int32_t* ipiv, int n, int32_t* perm, int32_t* work, cudaStream_t s);
 

@@ -140,6 +140,24 @@ __global__ void __launch_bounds__(1024) ipiv_to_perm_kernel(const int32_t* ipiv,
   }
 }
 
+// x <- P x in place for an ipiv vector (all swaps in order), using only
+// shared memory: batches of 256 pivots are composed and applied as one
+// gather/scatter each.
+__global__ void __launch_bounds__(1024) ipiv_apply_vector_kernel(const int32_t* ipiv, int n, double* x) {
+  __shared__ int p[256], nxt[256], lb[256];
+  __shared__ int dst[512], src[512];
+  __shared__ double vals[512];
+  __shared__ int s_m;
+  for (int k0 = 0; k0 < n; k0 += 256) {
+    const int cnt = min(256, n - k0);
+    const int m = compose_batch(ipiv, k0, cnt, p, nxt, lb, dst, src, &s_m);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) vals[i] = x[src[i]];
+    __syncthreads();
+    for (int i = threadIdx.x; i < m; i += blockDim.x) x[dst[i]] = vals[i];
+    __syncthreads();
+  }
+}
+
 template <typename T>
 constexpr int apply_cs() { return 128 / (int)sizeof(T); }  // 128-byte row segments
 
@@ -176,6 +194,13 @@ int launch_pivot_apply(T* A, int64_t lda, int c_begin, int c_end, int skip_begin
 
 int launch_ipiv_to_perm(const int32_t* ipiv, int n, int32_t* perm, int32_t* work, cudaStream_t s) {
   ipiv_to_perm_kernel<<<1, 1024, 0, s>>>(ipiv, n, perm, work);
+  LUB_LAUNCH_CHECK();
+  return LU_OK;
+}
+
+int launch_ipiv_apply_vector(const int32_t* ipiv, int n, double* x, cudaStream_t s) {
+  if (n <= 0) return LU_OK;
+  ipiv_apply_vector_kernel<<<1, 1024, 0, s>>>(ipiv, n, x);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }

@@ -209,6 +209,20 @@ LU_API int lu_phase_times(lu_handle h, double* ms, int64_t* launches, double* fl
 /* Kernels this library has launched since it was loaded (all handles). */
 LU_API int64_t lu_launch_count(void);
 
+/* Solve without allocating (no counterpart in the reference).  For callers
+ * that cannot call cudaMalloc — code running inside a CUDA graph capture, a
+ * host with a fixed device-memory budget, or a caller without a handle.
+ * Same result as lu_solve(h, dLU, lda, ipiv, db, 1, 1, 0, stream): x =
+ * A^{-1} b from lu_factor's factors and pivots, db (device) overwritten.
+ * Scratch lives in a fixed ~8 KB device array inside the library (held by
+ * every GPU that loads it until exit), so n is limited to 131072; larger n
+ * returns LU_ERR_ARG.  d_status (optional, device int) receives LU_OK or
+ * LU_ERR_TIMEOUT.  The first call on a device resolves the array's address
+ * and should come before any stream capture.  Calls share the array: calls
+ * that overlap on the GPU race. */
+LU_API int lu_solve_noalloc(const double* dLU, int64_t lda, int64_t n, const int32_t* ipiv, double* db,
+                            int32_t* d_status, void* stream);
+
 /* Message for a status code. */
 LU_API const char* lu_status_string(int status);
 
