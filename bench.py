@@ -161,6 +161,8 @@ def main():
     ap.add_argument("--n", type=int, default=65536)
     ap.add_argument("--block", type=int, default=256)
     ap.add_argument("--block-mixed", type=int, default=512)
+    ap.add_argument("--precision", default="fp16x3", choices=["bf16", "fp16s", "fp16x3"])
+    ap.add_argument("--lookahead", type=int, default=1)
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--mode", default="auto", choices=["auto", "fp64", "mixed"])
     ap.add_argument("--ref-sample", type=int, default=8192)
@@ -200,7 +202,7 @@ def main():
     rhs0 = lu.generate_uniform(n, 1, seed=seed, stream_id=1, device=dev).view(-1)
 
     # ---------------- FP64 path: factor_solve on a copy of A0 ----------------
-    s64 = lu.LUSolver(lu.LUConfig(n, b))
+    s64 = lu.LUSolver(lu.LUConfig(n, b, lookahead=bool(args.lookahead)))
     A = torch.empty_like(A0)
     x = torch.empty_like(rhs0)
 
@@ -214,7 +216,8 @@ def main():
             ev[1].record()
 
     # ---------------- mixed path: refine_solve (A0, b read only) -------------
-    smx = lu.LUSolver(lu.LUConfig(n, bm, precision=lu.LU_PREC_BF16)) if mode == "mixed" else None
+    prec = {"bf16": lu.LU_PREC_BF16, "fp16s": lu.LU_PREC_FP16S, "fp16x3": lu.LU_PREC_FP16X3}[args.precision]
+    smx = lu.LUSolver(lu.LUConfig(n, bm, precision=prec, lookahead=bool(args.lookahead))) if mode == "mixed" else None
     xm = torch.empty_like(rhs0)
     last_info = {}
 
@@ -309,7 +312,8 @@ def main():
     gemm_tf = gfl / gms / 1e9 if gms > 0 else None
     if mode == "mixed":
         peak_v = peaks.get("bf16_tflops_sustained") or 1376.1
-        roof = {"bound": "tensor", "kernel": "gemm_bf16_tc_kernel (trailing update, tcgen05 kind::f16, TMEM accum)",
+        roof = {"bound": "tensor", "kernel": f"gemm_bf16_tc_kernel (trailing update, tcgen05 kind::f16 {args.precision}, "
+                                             "TMEM accum; flops counted as executed, 3x for fp16x3)",
                 "achieved": gemm_tf, "peak": peak_v, "unit": "TFLOP/s",
                 "frac": (gemm_tf / peak_v) if gemm_tf else None, "traffic": None,
                 "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"}
@@ -332,12 +336,15 @@ def main():
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "bf16-tensor/f32-panel/f64-ir" if mode == "mixed" else "f64",
+            "dtype": (f"{args.precision}-tensor/f32-panel/f64-ir") if mode == "mixed" else "f64",
             "data": "synthetic uniform[-0.5,0.5) seed 42 (counter-based generator)",
-            "config": {"workload": (f"N={n} dense LU + solve to r_hpl<16: BF16-trailing/FP32-panel factor + FP64 "
-                                    f"refinement (b={bm}), FP64 LU (b={b}) beside it") if mode == "mixed" else
+            "config": {"workload": (f"N={n} dense LU + solve to r_hpl<16: {args.precision} tensor-core trailing update / "
+                                    f"FP32 panel factor + FP64 refinement (b={bm}), FP64 LU (b={b}) beside it; "
+                                    f"look-ahead={'on' if args.lookahead else 'off'}") if mode == "mixed" else
                        f"N={n} dense LU with partial pivoting + solve, FP64 path, b={b}",
                        "n": n, "block_size": bm if mode == "mixed" else b, "path": mode,
+                       "precision": args.precision if mode == "mixed" else "fp64",
+                       "lookahead": bool(args.lookahead),
                        "l2": "inputs 34 GB >> 126 MB L2 (no flush needed)",
                        "parallelism": "replicas" if world > 1 else "single"},
             "time_to_solution_s": tot_ms / args.steps / 1e3,

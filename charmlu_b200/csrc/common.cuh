@@ -112,6 +112,20 @@ __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target,
   return s_ok != 0;
 }
 
+// Grouped raster over an ntm x ntn tile grid: blocks run down groups of
+// `group` tile-rows before moving right, so the CTAs resident at one time
+// share a few A row-panels and B column-panels in L2 instead of streaming
+// the whole B operand once per tile-row.
+__device__ __forceinline__ void grouped_tile(int bid, int ntm, int ntn, int group, int& tm, int& tn) {
+  const int per_group = group * ntn;
+  const int g = bid / per_group;
+  const int first = g * group;
+  const int gs = min(ntm - first, group);
+  const int r = bid - g * per_group;
+  tm = first + r % gs;
+  tn = r / gs;
+}
+
 // ---------------------------------------------------------------------------
 // Counter-based generator (SplitMix64 finaliser); identical to the oracle's.
 // ---------------------------------------------------------------------------

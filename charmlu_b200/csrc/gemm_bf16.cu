@@ -117,7 +117,9 @@ gemm_bf16_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_const
   __shared__ int s_fail;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int tile_m = blockIdx.y * BM, tile_n = blockIdx.x * BN;
+  int tm, tn;
+  grouped_tile(blockIdx.x, (args.M + BM - 1) / BM, (args.N + BN - 1) / BN, 16, tm, tn);
+  const int tile_m = tm * BM, tile_n = tn * BN;
   const int KT = (args.K + BK - 1) / BK;
   const long long lim = args.spin >> 4;
 
@@ -230,8 +232,9 @@ int launch_gemm_bf16_tc(const CUtensorMap& mapA, const CUtensorMap& mapB, const 
   if (M <= 0 || N <= 0 || K <= 0) return LU_OK;
   if (c_col0 & 3) return LU_ERR_ALIGN;  // TMA x coordinate * 4 bytes must be a multiple of 16
   Bf16GemmArgs a{a_row0, b_row0, c_row0, c_col0, M, N, K, make_idesc(bf16), amax, st, spin};
-  dim3 grid(ceil_div(N, BN), ceil_div(M, BM));
-  gemm_bf16_tc_kernel<<<grid, THREADS, SMEM_BYTES, s>>>(mapA, mapB, mapC, a);
+  const int64_t tiles = (int64_t)ceil_div(N, BN) * ceil_div(M, BM);
+  if (tiles > INT32_MAX) return LU_ERR_UNSUPPORTED;
+  gemm_bf16_tc_kernel<<<(unsigned)tiles, THREADS, SMEM_BYTES, s>>>(mapA, mapB, mapC, a);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }

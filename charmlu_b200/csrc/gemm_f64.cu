@@ -55,7 +55,9 @@ gemm_f64_sub_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_const
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3;
   const int wm = warp >> 2, wn = warp & 3;
-  const int tile_m = blockIdx.y * BM, tile_n = blockIdx.x * BN;
+  int tm, tn;
+  grouped_tile(blockIdx.x, (args.M + BM - 1) / BM, (args.N + BN - 1) / BN, 16, tm, tn);
+  const int tile_m = tm * BM, tile_n = tn * BN;
   const int M = args.M, N = args.N, K = args.K;
   const int KT = (K + BK - 1) / BK;
 
@@ -218,8 +220,9 @@ int launch_gemm_f64_sub(const CUtensorMap& mapA, const CUtensorMap& mapB, const 
   if (a.M <= 0 || a.N <= 0 || a.K <= 0) return LU_OK;
   if ((a.a_col0 & 1) || (a.b_col0 & 1) || (a.ldc & 1) || (reinterpret_cast<uintptr_t>(a.C) & 15))
     return LU_ERR_ALIGN;
-  dim3 grid(ceil_div(a.N, BN), ceil_div(a.M, BM));
-  gemm_f64_sub_kernel<<<grid, THREADS, SMEM_BYTES, stream>>>(mapA, mapB, a);
+  const int64_t tiles = (int64_t)ceil_div(a.N, BN) * ceil_div(a.M, BM);
+  if (tiles > INT32_MAX) return LU_ERR_UNSUPPORTED;
+  gemm_f64_sub_kernel<<<(unsigned)tiles, THREADS, SMEM_BYTES, stream>>>(mapA, mapB, a);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }

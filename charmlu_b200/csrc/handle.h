@@ -42,7 +42,13 @@ struct lu_handle_s {
   int next_counter = 0;
   lub::LeafScratch<double> leaf64{};
   lub::LeafScratch<float> leaf32{};
-  lub::PivotList plist{};
+  lub::PivotList plist{};      // pivot lists of the trailing stream
+  lub::PivotList plistP{};     // pivot lists of the panel stream (look-ahead)
+  cudaStream_t sP = nullptr;   // high-priority panel stream (look-ahead)
+  cudaEvent_t evFork = nullptr, evP = nullptr, evN = nullptr;
+  // leaf tuning: recursion leaf width and CTA cap, without / with look-ahead
+  int leaf_w64 = 32, leaf_w32 = 64, leaf_ctas = 148;
+  int leaf_w64_la = 16, leaf_w32_la = 32, leaf_ctas_la = 64;
   int32_t* perm = nullptr;
   int32_t* perm_work = nullptr;
   int* trsv_flags = nullptr;

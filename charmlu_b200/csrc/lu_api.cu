@@ -95,6 +95,9 @@ struct Ctx64 {
   int n;
   cudaStream_t s;
   double thr;
+  PivotList pl;
+  int leaf_w;
+  int leaf_ctas;
 };
 
 int pivots_apply_f64(Ctx64& c, int k0, int cnt, int c_begin, int c_end, int skip_b, int skip_e, double* rhs,
@@ -102,9 +105,8 @@ int pivots_apply_f64(Ctx64& c, int k0, int cnt, int c_begin, int c_end, int skip
   Prof pf(c.h, c.s, LU_PH_LASWP);
   for (int off = 0; off < cnt; off += 512) {
     const int sub = std::min(512, cnt - off);
-    LUB_TRY(launch_pivot_compose(c.ipiv, k0 + off, sub, c.h->plist, c.s));
-    LUB_TRY(launch_pivot_apply<double>(c.A.p, c.A.ld, c_begin, c_end, skip_b, skip_e, c.h->plist, 2 * sub, rhs, perm,
-                                       c.s));
+    LUB_TRY(launch_pivot_compose(c.ipiv, k0 + off, sub, c.pl, c.s));
+    LUB_TRY(launch_pivot_apply<double>(c.A.p, c.A.ld, c_begin, c_end, skip_b, skip_e, c.pl, 2 * sub, rhs, perm, c.s));
   }
   return LU_OK;
 }
@@ -136,12 +138,12 @@ int trsm64(Ctx64& c, const MatF64& Lm, int r0, int w, const MatF64& Bm, int rb, 
 // recursive panel factorisation of columns [c0, c0+w), rows [c0, n)
 int panel64(Ctx64& c, int c0, int w) {
   const int M = c.n - c0;
-  if (w <= 32) {
+  if (w <= c.leaf_w) {
     unsigned* bar = c.h->take_counter();
     if (!bar) return LU_ERR_NOMEM;
     Prof pf(c.h, c.s, LU_PH_PANEL, (double)M * w * w);
     return launch_getf2_leaf<double>(c.A.at(c0, c0), c.A.ld, M, w, c.ipiv + c0, c0, c.h->leaf64, bar, c.h->st, c0,
-                                     c.thr, c.h->spin, c.h->num_sms, c.s);
+                                     c.thr, c.h->spin, c.leaf_ctas, c.s);
   }
   const int w1 = split_w(w), w2 = w - w1;
   LUB_TRY(panel64(c, c0, w1));
@@ -163,22 +165,54 @@ int factor_f64(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double* rhs,
   LUB_TRY(check_common(h, dA, lda));
   if (!ipiv) return LU_ERR_ARG;
   const int n = (int)h->cfg.n, b = h->cfg.block_size;
+  const bool la = h->cfg.lookahead != 0;
   Ctx64 c;
-  c.h = h; c.ipiv = ipiv; c.n = n; c.s = s; c.thr = h->cfg.sing_threshold;
+  c.h = h; c.ipiv = ipiv; c.n = n; c.s = s; c.thr = h->cfg.sing_threshold; c.pl = h->plist;
+  c.leaf_w = la ? h->leaf_w64_la : h->leaf_w64;
+  c.leaf_ctas = la ? h->leaf_ctas_la : h->leaf_ctas;
   LUB_TRY(c.A.init(dA, n, n, lda));
   LUB_CUDA(cudaMemsetAsync(h->st, 0, sizeof(DevStatus), s));
   LUB_CUDA(cudaMemsetAsync(h->counters, 0, sizeof(unsigned) * h->n_counters, s));
   h->next_counter = 0;
   LUB_TRY(launch_iota(h->perm, n, s));
-  for (int k0 = 0; k0 < n; k0 += b) {
-    const int kw = std::min(b, n - k0);
-    LUB_TRY(panel64(c, k0, kw));
-    LUB_TRY(pivots_apply_f64(c, k0, kw, 0, n, k0, k0 + kw, rhs, h->perm));
-    const int rest = n - k0 - kw;
-    if (rest > 0) {
-      LUB_TRY(trsm64(c, c.A, k0, kw, c.A, k0, k0 + kw, rest));
-      LUB_TRY(gemm64(c, c.A, k0 + kw, k0 + kw, c.A, k0 + kw, k0, c.A, k0, k0 + kw, rest, rest, kw, LU_PH_GEMM));
+  if (!la) {
+    for (int k0 = 0; k0 < n; k0 += b) {
+      const int kw = std::min(b, n - k0);
+      LUB_TRY(panel64(c, k0, kw));
+      LUB_TRY(pivots_apply_f64(c, k0, kw, 0, n, k0, k0 + kw, rhs, h->perm));
+      const int rest = n - k0 - kw;
+      if (rest > 0) {
+        LUB_TRY(trsm64(c, c.A, k0, kw, c.A, k0, k0 + kw, rest));
+        LUB_TRY(gemm64(c, c.A, k0 + kw, k0 + kw, c.A, k0 + kw, k0, c.A, k0, k0 + kw, rest, rest, kw, LU_PH_GEMM));
+      }
     }
+    return LU_OK;
+  }
+  // Look-ahead (replaces BlockScheduler's policy, scheduler.C:235-484, and the
+  // eager U solve next to the diagonal, lu.ci:141-145): panel k+1 runs on the
+  // high-priority panel stream as soon as the trailing update has reached its
+  // columns, while the rest of trailing update k runs on the caller's stream.
+  Ctx64 cp = c;
+  cp.s = h->sP;
+  cp.pl = h->plistP;
+  LUB_CUDA(cudaEventRecord(h->evFork, s));
+  LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evFork, 0));
+  LUB_TRY(panel64(cp, 0, std::min(b, n)));
+  LUB_CUDA(cudaEventRecord(h->evP, h->sP));
+  for (int k0 = 0; k0 < n; k0 += b) {
+    const int kw = std::min(b, n - k0), k1 = k0 + kw, rest = n - k1;
+    LUB_CUDA(cudaStreamWaitEvent(s, h->evP, 0));  // panel k factored (joins the panel stream)
+    LUB_TRY(pivots_apply_f64(c, k0, kw, 0, n, k0, k1, rhs, h->perm));
+    if (rest <= 0) continue;
+    LUB_TRY(trsm64(c, c.A, k0, kw, c.A, k0, k1, rest));
+    const int nw = std::min(b, rest);
+    LUB_TRY(gemm64(c, c.A, k1, k1, c.A, k1, k0, c.A, k0, k1, rest, nw, kw, LU_PH_GEMM));  // next panel's columns
+    LUB_CUDA(cudaEventRecord(h->evN, s));
+    LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evN, 0));
+    LUB_TRY(panel64(cp, k1, nw));
+    LUB_CUDA(cudaEventRecord(h->evP, h->sP));
+    if (rest > nw)
+      LUB_TRY(gemm64(c, c.A, k1, k1 + nw, c.A, k1, k0, c.A, k0, k1 + nw, rest, rest - nw, kw, LU_PH_GEMM));
   }
   return LU_OK;
 }
@@ -223,7 +257,7 @@ size_t lu_workspace_bytes(const lu_config* cfg) {
        2 * kMaxLeafW * sizeof(double);
   b += 2 * kMaxLeafCTAs * (sizeof(float) + sizeof(int)) + 2 * kMaxLeafCTAs * kMaxLeafW * sizeof(float) +
        2 * kMaxLeafW * sizeof(float);
-  b += sizeof(int32_t) * (4 * kMaxBatch + 1);
+  b += 2 * sizeof(int32_t) * (4 * kMaxBatch + 1);
   b += sizeof(int32_t) * 2 * n;
   b += sizeof(int) * (n / 64 + 2) + sizeof(unsigned);
   b += sizeof(double) * 2 * n;
@@ -257,6 +291,25 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
   if (s == LU_OK) s = h->alloc(&h->plist.dst, 2 * kMaxBatch);
   if (s == LU_OK) s = h->alloc(&h->plist.src, 2 * kMaxBatch);
   if (s == LU_OK) s = h->alloc(&h->plist.m, 1);
+  if (s == LU_OK) s = h->alloc(&h->plistP.dst, 2 * kMaxBatch);
+  if (s == LU_OK) s = h->alloc(&h->plistP.src, 2 * kMaxBatch);
+  if (s == LU_OK) s = h->alloc(&h->plistP.m, 1);
+  if (s == LU_OK) {
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    if (cudaStreamCreateWithPriority(&h->sP, cudaStreamNonBlocking, hi) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->evP, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->evN, cudaEventDisableTiming) != cudaSuccess)
+      s = LU_ERR_CUDA;
+  }
+  h->leaf_ctas = h->num_sms;
+  if (const char* e = getenv("LU_B200_LEAF_CTAS")) h->leaf_ctas = std::max(1, atoi(e));
+  if (const char* e = getenv("LU_B200_LEAF_CTAS_LA")) h->leaf_ctas_la = std::max(1, atoi(e));
+  if (const char* e = getenv("LU_B200_LEAF_W64")) h->leaf_w64 = std::min(32, std::max(2, atoi(e)));
+  if (const char* e = getenv("LU_B200_LEAF_W64_LA")) h->leaf_w64_la = std::min(32, std::max(2, atoi(e)));
+  if (const char* e = getenv("LU_B200_LEAF_W32")) h->leaf_w32 = std::min(64, std::max(4, atoi(e)));
+  if (const char* e = getenv("LU_B200_LEAF_W32_LA")) h->leaf_w32_la = std::min(64, std::max(4, atoi(e)));
   if (s == LU_OK) s = h->alloc(&h->perm, n);
   if (s == LU_OK) s = h->alloc(&h->perm_work, n);
   if (s == LU_OK) s = h->alloc(&h->trsv_flags, n / 64 + 2);
@@ -277,6 +330,10 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
 int lu_destroy(lu_handle h) {
   if (!h) return LU_ERR_ARG;
   for (cudaEvent_t e : h->pool) cudaEventDestroy(e);
+  if (h->evFork) cudaEventDestroy(h->evFork);
+  if (h->evP) cudaEventDestroy(h->evP);
+  if (h->evN) cudaEventDestroy(h->evN);
+  if (h->sP) cudaStreamDestroy(h->sP);
   for (void* p : h->allocs) cudaFree(p);
   if (h->racc_host) cudaFreeHost(h->racc_host);
   delete h;

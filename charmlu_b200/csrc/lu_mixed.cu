@@ -56,6 +56,9 @@ struct Ctx32 {
   int32_t* ipiv;
   cudaStream_t s;
   double thr;
+  PivotList pl;
+  int leaf_w;
+  int leaf_ctas;
 };
 
 inline int split_w32(int w) {
@@ -68,9 +71,8 @@ int pivots_apply_f32(Ctx32& c, int k0, int cnt, int c_begin, int c_end, int skip
   Prof pf(c.h, c.s, LU_PH_LASWP);
   for (int off = 0; off < cnt; off += 512) {
     const int sub = std::min(512, cnt - off);
-    LUB_TRY(launch_pivot_compose(c.ipiv, k0 + off, sub, c.h->plist, c.s));
-    LUB_TRY(launch_pivot_apply<float>(c.A, c.ld, c_begin, c_end, skip_b, skip_e, c.h->plist, 2 * sub, nullptr, perm,
-                                      c.s));
+    LUB_TRY(launch_pivot_compose(c.ipiv, k0 + off, sub, c.pl, c.s));
+    LUB_TRY(launch_pivot_apply<float>(c.A, c.ld, c_begin, c_end, skip_b, skip_e, c.pl, 2 * sub, nullptr, perm, c.s));
   }
   return LU_OK;
 }
@@ -95,12 +97,12 @@ int trsm32(Ctx32& c, int r0, int w, int rb, int cb, int ncols) {
 
 int panel32(Ctx32& c, int c0, int w) {
   const int M = c.n - c0;
-  if (w <= 64) {
+  if (w <= c.leaf_w) {
     unsigned* bar = c.h->take_counter();
     if (!bar) return LU_ERR_NOMEM;
     Prof pf(c.h, c.s, LU_PH_PANEL, (double)M * w * w);
     return launch_getf2_leaf<float>(c.A + (int64_t)c0 * c.ld + c0, c.ld, M, w, c.ipiv + c0, c0, c.h->leaf32, bar,
-                                    c.h->st, c0, c.thr, c.h->spin, c.h->num_sms, c.s);
+                                    c.h->st, c0, c.thr, c.h->spin, c.leaf_ctas, c.s);
   }
   const int w1 = split_w32(w), w2 = w - w1;
   LUB_TRY(panel32(c, c0, w1));
@@ -111,48 +113,91 @@ int panel32(Ctx32& c, int c0, int w) {
   return pivots_apply_f32(c, c0 + w1, w2, c0, c0 + w1, 0, 0, nullptr);
 }
 
-// LU of h->A32 in place: FP32 panels/TRSM, BF16 tcgen05 trailing updates.
+// Low-precision operand panels of step k (L21 rows k1.., U12^T) and their
+// tensor maps; K' = nparts * kw.
+int build_operands(lu_handle h, const Ctx32& c, int k0, int kw, int k1, int rest, bool bf16, CUtensorMap* mapL,
+                   CUtensorMap* mapU, cudaStream_t s) {
+  const float* L21 = c.A + (int64_t)k1 * c.ld + k0;
+  const float* U12 = c.A + (int64_t)k0 * c.ld + k1;
+  const int ke = h->nparts * kw;
+  {
+    Prof pf(h, s, LU_PH_OTHER);
+    if (bf16) {
+      LUB_TRY(launch_split_rows<__nv_bfloat16>(L21, c.ld, h->Lb, h->ldk, rest, kw, 1, 0u, nullptr, 0, s));
+      LUB_TRY(launch_split_transpose<__nv_bfloat16>(U12, c.ld, h->Ub, h->ldk, kw, rest, 1, 0u, nullptr, 1, s));
+    } else {
+      // L parts [hi, hi, lo] against U parts [hi, lo, hi]: Lh*Uh + Lh*Ul + Ll*Uh
+      LUB_TRY(launch_panel_absmax(L21, c.ld, rest, kw, U12, c.ld, rest, h->amax, s));
+      LUB_TRY(launch_split_rows<__half>(L21, c.ld, reinterpret_cast<__half*>(h->Lb), h->ldk, rest, kw, h->nparts,
+                                        0x4u, h->amax, 0, s));
+      LUB_TRY(launch_split_transpose<__half>(U12, c.ld, reinterpret_cast<__half*>(h->Ub), h->ldk, kw, rest,
+                                             h->nparts, 0x2u, h->amax, 1, s));
+    }
+  }
+  const CUtensorMapDataType dt = bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+  LUB_TRY(encode_tmap_2d(mapL, dt, 2, h->Lb, ke, rest, h->ldk * 2, 64, 128, CU_TENSOR_MAP_SWIZZLE_128B));
+  LUB_TRY(encode_tmap_2d(mapU, dt, 2, h->Ub, ke, rest, h->ldk * 2, 64, 256, CU_TENSOR_MAP_SWIZZLE_128B));
+  return LU_OK;
+}
+
+// C(k1.., c0..c0+ncols) -= L21 * U12[:, u0..u0+ncols] on the tensor cores
+int lowp_gemm(lu_handle h, const CUtensorMap& mapL, const CUtensorMap& mapU, const CUtensorMap& mapC, int k1,
+              int rest, int u0, int ncols, int ke, bool bf16, cudaStream_t s) {
+  Prof pf(h, s, LU_PH_GEMM, 2.0 * rest * (double)ncols * ke);
+  return launch_gemm_bf16_tc(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, ke, bf16, bf16 ? nullptr : h->amax,
+                             h->st, h->spin, s);
+}
+
+// LU of h->A32 in place: FP32 panels/TRSM, low-precision tcgen05 trailing
+// updates; with look-ahead, panel k+1 overlaps the rest of update k.
 int factor_mixed(lu_handle h, cudaStream_t s) {
   const int n = (int)h->cfg.n, B = h->cfg.block_size;
   const bool bf16 = h->cfg.precision == LU_PREC_BF16;
-  Ctx32 c{h, h->A32, h->ld32, n, h->ipiv32, s, h->cfg.sing_threshold};
+  const bool la = h->cfg.lookahead != 0;
+  Ctx32 c{h, h->A32, h->ld32, n, h->ipiv32, s, h->cfg.sing_threshold, h->plist,
+          la ? h->leaf_w32_la : h->leaf_w32, la ? h->leaf_ctas_la : h->leaf_ctas};
   CUtensorMap mapC;
   LUB_TRY(encode_tmap_2d(&mapC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->A32, n, n, h->ld32 * 4, 32, 128,
                          CU_TENSOR_MAP_SWIZZLE_128B));
   LUB_CUDA(cudaMemsetAsync(h->counters, 0, sizeof(unsigned) * h->n_counters, s));
   h->next_counter = 0;
   LUB_TRY(launch_iota(h->perm, n, s));
+  if (!la) {
+    for (int k0 = 0; k0 < n; k0 += B) {
+      const int kw = std::min(B, n - k0);
+      LUB_TRY(panel32(c, k0, kw));
+      LUB_TRY(pivots_apply_f32(c, k0, kw, 0, n, k0, k0 + kw, h->perm));
+      const int k1 = k0 + kw, rest = n - k1;
+      if (rest <= 0) continue;
+      LUB_TRY(trsm32(c, k0, kw, k0, k1, rest));
+      CUtensorMap mapL, mapU;
+      LUB_TRY(build_operands(h, c, k0, kw, k1, rest, bf16, &mapL, &mapU, s));
+      LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, 0, rest, h->nparts * kw, bf16, s));
+    }
+    return LU_OK;
+  }
+  Ctx32 cp = c;
+  cp.s = h->sP;
+  cp.pl = h->plistP;
+  LUB_CUDA(cudaEventRecord(h->evFork, s));
+  LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evFork, 0));
+  LUB_TRY(panel32(cp, 0, std::min(B, n)));
+  LUB_CUDA(cudaEventRecord(h->evP, h->sP));
   for (int k0 = 0; k0 < n; k0 += B) {
-    const int kw = std::min(B, n - k0);
-    LUB_TRY(panel32(c, k0, kw));
-    LUB_TRY(pivots_apply_f32(c, k0, kw, 0, n, k0, k0 + kw, h->perm));
-    const int k1 = k0 + kw, rest = n - k1;
+    const int kw = std::min(B, n - k0), k1 = k0 + kw, rest = n - k1;
+    LUB_CUDA(cudaStreamWaitEvent(s, h->evP, 0));
+    LUB_TRY(pivots_apply_f32(c, k0, kw, 0, n, k0, k1, h->perm));
     if (rest <= 0) continue;
     LUB_TRY(trsm32(c, k0, kw, k0, k1, rest));
-    const float* L21 = c.A + (int64_t)k1 * c.ld + k0;
-    const float* U12 = c.A + (int64_t)k0 * c.ld + k1;
-    const int ke = h->nparts * kw;  // K of the low-precision product (3 K-blocks for the split)
-    {
-      Prof pf(h, s, LU_PH_OTHER);
-      if (bf16) {
-        LUB_TRY(launch_split_rows<__nv_bfloat16>(L21, c.ld, h->Lb, h->ldk, rest, kw, 1, 0u, nullptr, 0, s));
-        LUB_TRY(launch_split_transpose<__nv_bfloat16>(U12, c.ld, h->Ub, h->ldk, kw, rest, 1, 0u, nullptr, 1, s));
-      } else {
-        // L parts [hi, hi, lo] against U parts [hi, lo, hi]: Lh*Uh + Lh*Ul + Ll*Uh
-        LUB_TRY(launch_panel_absmax(L21, c.ld, rest, kw, U12, c.ld, rest, h->amax, s));
-        LUB_TRY(launch_split_rows<__half>(L21, c.ld, reinterpret_cast<__half*>(h->Lb), h->ldk, rest, kw, h->nparts,
-                                          0x4u, h->amax, 0, s));
-        LUB_TRY(launch_split_transpose<__half>(U12, c.ld, reinterpret_cast<__half*>(h->Ub), h->ldk, kw, rest,
-                                               h->nparts, 0x2u, h->amax, 1, s));
-      }
-    }
-    const CUtensorMapDataType dt = bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
     CUtensorMap mapL, mapU;
-    LUB_TRY(encode_tmap_2d(&mapL, dt, 2, h->Lb, ke, rest, h->ldk * 2, 64, 128, CU_TENSOR_MAP_SWIZZLE_128B));
-    LUB_TRY(encode_tmap_2d(&mapU, dt, 2, h->Ub, ke, rest, h->ldk * 2, 64, 256, CU_TENSOR_MAP_SWIZZLE_128B));
-    Prof pf(h, s, LU_PH_GEMM, 2.0 * rest * (double)rest * ke);
-    LUB_TRY(launch_gemm_bf16_tc(mapL, mapU, mapC, 0, 0, k1, k1, rest, rest, ke, bf16, bf16 ? nullptr : h->amax,
-                                h->st, h->spin, s));
+    LUB_TRY(build_operands(h, c, k0, kw, k1, rest, bf16, &mapL, &mapU, s));
+    const int nw = std::min(B, rest), ke = h->nparts * kw;
+    LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, 0, nw, ke, bf16, s));  // next panel's columns
+    LUB_CUDA(cudaEventRecord(h->evN, s));
+    LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evN, 0));
+    LUB_TRY(panel32(cp, k1, nw));
+    LUB_CUDA(cudaEventRecord(h->evP, h->sP));
+    if (rest > nw) LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, nw, rest - nw, ke, bf16, s));
   }
   return LU_OK;
 }

@@ -174,41 +174,56 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
   }
 }
 
-template <typename T>
-constexpr int leaf_w() { return sizeof(T) == 8 ? 32 : 64; }
+template <typename T, int W>
+size_t leaf_smem(int R) { return (size_t)R * (W + 1) * sizeof(T) + W * sizeof(T); }
 
-template <typename T>
-size_t leaf_smem(int R) { return (size_t)R * (leaf_w<T>() + 1) * sizeof(T) + leaf_w<T>() * sizeof(T); }
-
-}  // namespace
-
-template <typename T>
-int leaf_init() {
-  LUB_CUDA(cudaFuncSetAttribute(getf2_leaf_kernel<T, leaf_w<T>()>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                220 * 1024));
-  return LU_OK;
-}
-
-template <typename T>
-int launch_getf2_leaf(T* P, int64_t lda, int M, int ncols, int32_t* ipiv, int row_base, const LeafScratch<T>& scr,
-                      unsigned* bar, DevStatus* st, int info_base, double thr, long long spin, int max_ctas,
-                      cudaStream_t s) {
-  constexpr int W = leaf_w<T>();
-  if (M <= 0 || ncols <= 0) return LU_OK;
-  if (ncols > W) return LU_ERR_ARG;
-  // rows per CTA: enough CTAs to spread the panel, capped by the SM count
-  // and by shared memory (R * (W+1) * sizeof(T) <= ~216 KB)
+template <typename T, int W>
+int launch_leaf_w(T* P, int64_t lda, int M, int ncols, int32_t* ipiv, int row_base, const LeafScratch<T>& scr,
+                  unsigned* bar, DevStatus* st, int info_base, double thr, long long spin, int max_ctas,
+                  cudaStream_t s) {
+  // rows per CTA: enough CTAs to spread the panel, capped by max_ctas and by
+  // shared memory (R * (W+1) * sizeof(T) <= ~216 KB)
   const int max_rows = (int)((216 * 1024 - W * sizeof(T)) / ((W + 1) * sizeof(T)));
   int G = std::min(std::max(ceil_div(M, 256), 1), std::min(max_ctas, kMaxLeafCTAs));
   int R = ceil_div(M, G);
-  if (R > max_rows) return LU_ERR_UNSUPPORTED;
+  if (R > max_rows) {  // too few CTAs allowed for this height: take what shared memory needs
+    R = max_rows;
+    G = ceil_div(M, R);
+    if (G > kMaxLeafCTAs) return LU_ERR_UNSUPPORTED;
+  }
   G = ceil_div(M, R);
-  size_t smem = leaf_smem<T>(R);
+  size_t smem = leaf_smem<T, W>(R);
   void* args[] = {&P, &lda, &M, &ncols, &R, &ipiv, &row_base, const_cast<LeafScratch<T>*>(&scr), &bar, &st,
                   &info_base, &thr, &spin};
   LUB_CUDA(cudaLaunchCooperativeKernel((const void*)getf2_leaf_kernel<T, W>, dim3(G), dim3(THREADS), args, smem, s));
   __atomic_add_fetch(&g_kernel_launches, 1, __ATOMIC_RELAXED);
   return LU_OK;
+}
+
+}  // namespace
+
+template <typename T>
+int leaf_init() {
+  LUB_CUDA(cudaFuncSetAttribute(getf2_leaf_kernel<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+  LUB_CUDA(cudaFuncSetAttribute(getf2_leaf_kernel<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+  LUB_CUDA(cudaFuncSetAttribute(getf2_leaf_kernel<T, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+  return LU_OK;
+}
+
+// ncols <= 64; the kernel instance is the narrowest of 16/32/64 that holds
+// ncols, so narrow leaves keep more rows per CTA and need fewer CTAs.
+template <typename T>
+int launch_getf2_leaf(T* P, int64_t lda, int M, int ncols, int32_t* ipiv, int row_base, const LeafScratch<T>& scr,
+                      unsigned* bar, DevStatus* st, int info_base, double thr, long long spin, int max_ctas,
+                      cudaStream_t s) {
+  if (M <= 0 || ncols <= 0) return LU_OK;
+  if (ncols <= 16)
+    return launch_leaf_w<T, 16>(P, lda, M, ncols, ipiv, row_base, scr, bar, st, info_base, thr, spin, max_ctas, s);
+  if (ncols <= 32)
+    return launch_leaf_w<T, 32>(P, lda, M, ncols, ipiv, row_base, scr, bar, st, info_base, thr, spin, max_ctas, s);
+  if (ncols <= 64)
+    return launch_leaf_w<T, 64>(P, lda, M, ncols, ipiv, row_base, scr, bar, st, info_base, thr, spin, max_ctas, s);
+  return LU_ERR_ARG;
 }
 
 template int leaf_init<double>();

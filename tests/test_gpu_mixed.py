@@ -77,7 +77,7 @@ def test_gemm_lowp_tcgen05_matches_reference(cuda_dev, M, N, K, mode):
         assert (split - A.double() @ B.double()).abs().max().item() <= 1e-5 * 18.5 * K / 64
 
 
-def _refine(n, b, A_np=None, seed=42, mode=None, target=16.0, prec=None):
+def _refine(n, b, A_np=None, seed=42, mode=None, target=16.0, prec=None, lookahead=False):
     import charmlu_b200 as lu
     prec = lu.LU_PREC_FP16X3 if prec is None else prec
     if A_np is None:
@@ -85,7 +85,7 @@ def _refine(n, b, A_np=None, seed=42, mode=None, target=16.0, prec=None):
     else:
         A = torch.from_numpy(A_np).cuda()
     rhs = lu.generate_uniform(n, 1, seed=seed, stream_id=1).view(-1)
-    cfg = lu.LUConfig(n, b, precision=prec, ir_target=target)
+    cfg = lu.LUConfig(n, b, precision=prec, ir_target=target, lookahead=lookahead)
     if mode is not None:
         cfg.ir_mode = mode
     s = lu.LUSolver(cfg)
@@ -134,3 +134,10 @@ def test_singular_matrix_reports_info_mixed(cuda_dev):
     A[:, 100] = 0.0
     s, Ad, rhs, x, info, st = _refine(n, b, A_np=A)
     assert st == 101, (st, info)
+
+
+@pytest.mark.parametrize("n,b", [(2048, 256), (4096, 512)])
+def test_refine_lookahead(cuda_dev, n, b):
+    s, A, rhs, x, info, st = _refine(n, b, lookahead=True)
+    assert st == 0 and info["status"] == 0, info
+    assert s.residual(A, x, rhs)["r_hpl"] < 16
