@@ -184,6 +184,28 @@ class LUSolver:
                "lu_residual")
         return {k: getattr(info, k) for k, _ in info._fields_}
 
+    def adjoint(self, LU, ipiv, X, W, gradB=None, gradA=None, want_gradA=True, stream=None):
+        """Adjoint of X = A^{-1} B (no reference counterpart): lambda =
+        A^{-T} W into gradB, grad_A = -lambda X^T into gradA (lu_adjoint).
+        Returns (gradA or None, gradB)."""
+        lda = self._check_matrix(LU)
+        n = self.n
+        for t, nm in ((X, "X"), (W, "W")):
+            _require_cuda(t, torch.float64, nm)
+        X2 = X if X.dim() == 2 else X.view(-1, 1)
+        W2 = W.contiguous() if W.dim() == 2 else W.contiguous().view(-1, 1)
+        k = W2.shape[1]
+        if gradB is None:
+            gradB = torch.empty(n, k, dtype=torch.float64, device=LU.device)
+        if want_gradA and gradA is None:
+            gradA = torch.empty(n, n, dtype=torch.float64, device=LU.device)
+        gB = gradB if gradB.dim() == 2 else gradB.view(-1, 1)
+        _check(self._L.lu_adjoint(self._h, _ptr(LU), lda, _ptr(ipiv), _ptr(X2), X2.stride(0) if k > 1 else 1,
+                                  _ptr(W2), W2.stride(0) if k > 1 else 1, k, _ptr(gB), gB.stride(0) if k > 1 else 1,
+                                  _ptr(gradA) if want_gradA else None, gradA.stride(0) if want_gradA else n,
+                                  _stream(stream)), "lu_adjoint")
+        return (gradA if want_gradA else None), gradB
+
     def profile(self, enable=True):
         """Bracket every phase of later calls with CUDA events (lu_profile)."""
         _check(self._L.lu_profile(self._h, int(bool(enable))), "lu_profile")

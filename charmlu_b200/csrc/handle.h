@@ -55,6 +55,8 @@ struct lu_handle_s {
   unsigned* trsv_ticket = nullptr;
   double* vec = nullptr;
   double* vec2 = nullptr;
+  double* tmpB = nullptr;      // n x nrhs staging block of multi-RHS solves (grown on demand)
+  size_t tmpB_elems = 0;
   lub::ResidualAccum* racc = nullptr;
   lub::ResidualAccum* racc_host = nullptr;
   // mixed-precision workspace (allocated on first use)

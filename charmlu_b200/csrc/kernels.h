@@ -69,6 +69,17 @@ template <typename T>
 int launch_trsv(const T* LU, int64_t lda, int n, T* x, int upper, int* flags, unsigned* ticket, DevStatus* st,
                 long long spin, cudaStream_t s);
 
+// multi-RHS pipelined triangular solve (mode 0 L, 1 U, 2 U^T, 3 L^T) on a
+// row-major n x nrhs block
+int launch_trsm_pipe(const double* LU, int64_t lda, int n, double* Y, int64_t ldy, int nrhs, int mode, int* flags,
+                     unsigned* ticket, DevStatus* st, long long spin, cudaStream_t s);
+// G = -Lam X^T (rank k <= 16)
+int launch_neg_outer(const double* Lam, int64_t ldl, const double* X, int64_t ldx, int n, int k, double* G,
+                     int64_t ldg, cudaStream_t s);
+// row permutation of an n x k block: gather Y[i] = X[perm[i]] or scatter Y[perm[i]] = X[i]
+int launch_permute_rows(const double* X, int64_t ldx, double* Y, int64_t ldy, const int32_t* perm, int n, int k,
+                        int scatter, cudaStream_t s);
+
 // ---- residual / GEMV / generators
 struct ResidualAccum {  // non-negative doubles stored as ordered bit patterns
   unsigned long long amax, anorm, bmax, xmax, rmax;

@@ -355,17 +355,59 @@ int lu_factor(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double* rhs, 
   return factor_f64(h, dA, lda, ipiv, rhs, (cudaStream_t)stream);
 }
 
+// n x nrhs staging block owned by the handle
+static int ensure_tmpB(lu_handle h, size_t elems) {
+  if (h->tmpB_elems >= elems) return LU_OK;
+  if (h->tmpB) {
+    cudaFree(h->tmpB);
+    h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->tmpB), h->allocs.end());
+    h->tmpB = nullptr;
+  }
+  LUB_TRY(h->alloc(&h->tmpB, elems));
+  h->tmpB_elems = elems;
+  return LU_OK;
+}
+
+// A^T Y = B with P A = L U  ->  U^T L^T (P Y) = B: solve U^T, then L^T on a
+// copy of B, then Y = P^T (that): rows scattered through the permutation.
+static int solve_trans_multi(lu_handle h, const double* dLU, int64_t lda, const double* B, int64_t ldb, int nrhs,
+                             double* Y, int64_t ldy, cudaStream_t s) {
+  const int n = (int)h->cfg.n;
+  LUB_TRY(ensure_tmpB(h, (size_t)n * nrhs));
+  LUB_CUDA(cudaMemcpy2DAsync(h->tmpB, sizeof(double) * nrhs, B, sizeof(double) * ldb, sizeof(double) * nrhs, n,
+                             cudaMemcpyDeviceToDevice, s));
+  Prof pf(h, s, LU_PH_SOLVE, 2.0 * n * (double)n * nrhs);
+  LUB_TRY(launch_trsm_pipe(dLU, lda, n, h->tmpB, nrhs, nrhs, 2, h->trsv_flags, h->trsv_ticket, h->st, h->spin, s));
+  LUB_TRY(launch_trsm_pipe(dLU, lda, n, h->tmpB, nrhs, nrhs, 3, h->trsv_flags, h->trsv_ticket, h->st, h->spin, s));
+  return launch_permute_rows(h->tmpB, nrhs, Y, ldy, h->perm_work, n, nrhs, 1, s);
+}
+
 int lu_solve(lu_handle h, const double* dLU, int64_t lda, const int32_t* ipiv, double* dB, int64_t ldb,
              int64_t nrhs, int trans, void* stream) {
   LUB_TRY(check_common(h, dLU, lda));
-  if (!ipiv || !dB || nrhs < 1 || ldb < nrhs) return LU_ERR_ARG;
-  if (trans != 0 || nrhs != 1) return LU_ERR_UNSUPPORTED;
+  if (!ipiv || !dB || nrhs < 1 || ldb < nrhs || (trans != 0 && trans != 1)) return LU_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   const int n = (int)h->cfg.n;
   LUB_TRY(launch_ipiv_to_perm(ipiv, n, h->perm_work, nullptr, s));
-  LUB_TRY(launch_gather_perm(dB, h->perm_work, h->vec, n, s));
-  LUB_TRY(solve_permuted_f64(h, dLU, lda, h->vec, s));
-  LUB_CUDA(cudaMemcpyAsync(dB, h->vec, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  if (trans == 0 && nrhs == 1) {
+    LUB_TRY(launch_gather_perm(dB, h->perm_work, h->vec, n, s));
+    LUB_TRY(solve_permuted_f64(h, dLU, lda, h->vec, s));
+    LUB_CUDA(cudaMemcpyAsync(dB, h->vec, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    return LU_OK;
+  }
+  if (trans == 1) return solve_trans_multi(h, dLU, lda, dB, ldb, (int)nrhs, dB, ldb, s);
+  // A X = B, several right-hand sides: gather P B, then L, then U
+  LUB_TRY(ensure_tmpB(h, (size_t)n * nrhs));
+  LUB_TRY(launch_permute_rows(dB, ldb, h->tmpB, nrhs, h->perm_work, n, (int)nrhs, 0, s));
+  {
+    Prof pf(h, s, LU_PH_SOLVE, 2.0 * n * (double)n * nrhs);
+    LUB_TRY(launch_trsm_pipe(dLU, lda, n, h->tmpB, nrhs, (int)nrhs, 0, h->trsv_flags, h->trsv_ticket, h->st,
+                             h->spin, s));
+    LUB_TRY(launch_trsm_pipe(dLU, lda, n, h->tmpB, nrhs, (int)nrhs, 1, h->trsv_flags, h->trsv_ticket, h->st,
+                             h->spin, s));
+  }
+  LUB_CUDA(cudaMemcpy2DAsync(dB, sizeof(double) * ldb, h->tmpB, sizeof(double) * nrhs, sizeof(double) * nrhs, n,
+                             cudaMemcpyDeviceToDevice, s));
   return LU_OK;
 }
 
@@ -402,12 +444,24 @@ int lu_residual(lu_handle h, const double* dA, int64_t lda, const double* dx, co
   return LU_OK;
 }
 
+// Adjoint of X = A^{-1} B for a loss with upstream gradient W = dL/dX:
+// lambda = A^{-T} W (the transposed triangular solves on the stored
+// factors), grad_B = lambda, grad_A = -lambda X^T (rank-nrhs product).
 int lu_adjoint(lu_handle h, const double* dLU, int64_t lda, const int32_t* ipiv, const double* dX, int64_t ldx,
                const double* dW, int64_t ldw, int64_t nrhs, double* gradB, int64_t ldgb, double* gradA,
                int64_t ldga, void* stream) {
-  (void)h; (void)dLU; (void)lda; (void)ipiv; (void)dX; (void)ldx; (void)dW; (void)ldw; (void)nrhs; (void)gradB;
-  (void)ldgb; (void)gradA; (void)ldga; (void)stream;
-  return LU_ERR_UNSUPPORTED;
+  LUB_TRY(check_common(h, dLU, lda));
+  const int64_t n = h->cfg.n;
+  if (!ipiv || !dW || !gradB || nrhs < 1 || ldw < nrhs || ldgb < nrhs) return LU_ERR_ARG;
+  if (gradA && (!dX || ldx < nrhs || ldga < n)) return LU_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  LUB_TRY(launch_ipiv_to_perm(ipiv, (int)n, h->perm_work, nullptr, s));
+  LUB_TRY(solve_trans_multi(h, dLU, lda, dW, ldw, (int)nrhs, gradB, ldgb, s));
+  if (gradA) {
+    Prof pf(h, s, LU_PH_OTHER, 2.0 * n * (double)n * nrhs);
+    LUB_TRY(launch_neg_outer(gradB, ldgb, dX, ldx, (int)n, (int)nrhs, gradA, ldga, s));
+  }
+  return LU_OK;
 }
 
 int lu_batched_factor_solve(int32_t count, const int32_t* n, const int64_t* a_off, const int64_t* b_off, double* dA,
