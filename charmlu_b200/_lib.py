@@ -12,7 +12,7 @@ LIB_PATH = os.path.join(HERE, "liblu_b200.so")
 LU_OK = 0
 LU_ERR_ARG, LU_ERR_CUDA, LU_ERR_TIMEOUT, LU_ERR_NONFINITE = -1, -2, -3, -4
 LU_ERR_NOCONV, LU_ERR_ALIGN, LU_ERR_NOMEM, LU_ERR_UNSUPPORTED = -5, -6, -7, -8
-LU_PREC_FP64, LU_PREC_BF16, LU_PREC_FP16S, LU_PREC_FP16X3 = 0, 1, 2, 3
+LU_PREC_FP64, LU_PREC_BF16, LU_PREC_FP16S, LU_PREC_FP16X3, LU_PREC_FP32 = 0, 1, 2, 3, 4
 LU_IR_CLASSIC, LU_IR_GMRES = 0, 1
 
 # every symbol the header declares (checked by the CPU test suite)
@@ -21,6 +21,7 @@ EXPORTS = [
     "lu_solve", "lu_factor_solve", "lu_residual", "lu_refine_solve", "lu_adjoint",
     "lu_batched_factor_solve", "lu_generate_uniform", "lu_matgen_host", "lu_status_string",
     "lu_profile", "lu_phase_times", "lu_launch_count", "lu_solve_noalloc",
+    "lu_batched_work_bytes", "lu_batched_set_tuning",
 ]
 PHASES = ["panel", "laswp", "trsm", "gemm", "gemm_inner", "solve", "other"]
 
@@ -77,6 +78,8 @@ def load():
         "lu_phase_times": ([H, P, P, P], ctypes.c_int),
         "lu_launch_count": ([], ctypes.c_int64),
         "lu_solve_noalloc": ([P, i64, i64, P, P, P, P], ctypes.c_int),
+        "lu_batched_work_bytes": ([i32, P, i32], ctypes.c_size_t),
+        "lu_batched_set_tuning": ([i32, P], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

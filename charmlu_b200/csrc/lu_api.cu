@@ -464,14 +464,6 @@ int lu_adjoint(lu_handle h, const double* dLU, int64_t lda, const int32_t* ipiv,
   return LU_OK;
 }
 
-int lu_batched_factor_solve(int32_t count, const int32_t* n, const int64_t* a_off, const int64_t* b_off, double* dA,
-                            double* db, int32_t* info, int32_t precision, void* dWork, size_t work_bytes,
-                            void* stream) {
-  (void)count; (void)n; (void)a_off; (void)b_off; (void)dA; (void)db; (void)info; (void)precision; (void)dWork;
-  (void)work_bytes; (void)stream;
-  return LU_ERR_UNSUPPORTED;
-}
-
 int lu_generate_uniform(double* d, int64_t rows, int64_t cols, int64_t ld, uint64_t seed, uint64_t stream_id,
                         void* stream) {
   if (!d || rows < 0 || cols < 0 || ld < cols) return LU_ERR_ARG;

@@ -168,16 +168,27 @@ LU_API int lu_adjoint(lu_handle h, const double* dLU, int64_t lda, const int32_t
                double* gradB, int64_t ldgb, double* gradA, int64_t ldga, void* stream);
 
 /* Batched factor+solve of many independent systems of uneven order in one
- * persistent launch (no reference counterpart).  System i has order n[i],
- * its matrix at dA + a_off[i] (row-major, lda = n[i]) and right-hand side
- * at db + b_off[i] (overwritten by x).  precision LU_PREC_FP64, or
- * LU_PREC_BF16 meaning FP32 factors plus one FP64 refinement step (then
- * dA must stay intact: factors go to the handle-free scratch dWork of
- * 4*sum(n^2) bytes).  info[i] receives each system's status.  All arrays
- * are device memory. */
+ * persistent launch (no reference counterpart).  System i has order n[i]
+ * (1 <= n[i] <= 1536), its matrix at dA + a_off[i] (row-major, lda = n[i])
+ * and right-hand side at db + b_off[i] (overwritten by x).  precision:
+ *   LU_PREC_FP64  FP64 factors in place in dA (as lu_factor);
+ *   LU_PREC_FP32  FP32 factors of a copy in dWork, then FP64 refinement
+ *                 against the untouched FP64 A until r_hpl < 16 (at most 4
+ *                 steps; LU_ERR_NOCONV in info[i] otherwise).
+ * info[i] receives each system's status (0 or 1-based singular column).
+ * dWork: device scratch of lu_batched_work_bytes(...) bytes.  All pointer
+ * arguments are device memory. */
+#define LU_PREC_FP32   4   /* batched only: FP32 factors + FP64 refinement steps */
 LU_API int lu_batched_factor_solve(int32_t count, const int32_t* n, const int64_t* a_off,
                             const int64_t* b_off, double* dA, double* db, int32_t* info,
                             int32_t precision, void* dWork, size_t work_bytes, void* stream);
+/* Scratch bytes lu_batched_factor_solve needs for these orders (n_host: host array). */
+LU_API size_t lu_batched_work_bytes(int32_t count, const int32_t* n_host, int32_t precision);
+/* Per-size-bucket kernel parameters chosen by the autotuner: entries of
+ * {n_max, panel_width, small_threshold} (host array, ascending n_max, at most
+ * 16); count 0 restores the built-in defaults.  Applies to later batched
+ * calls in this process. */
+LU_API int lu_batched_set_tuning(int32_t entries, const int32_t* table);
 
 /* Generators (device).  Counter-based uniform[-0.5,0.5): element (i, j)
  * of stream s is a pure function of (seed, s, i*cols + j), identical to
