@@ -16,10 +16,10 @@ import torch
 
 from . import _lib
 from ._lib import (LU_ERR_ARG, LU_ERR_NOCONV, LU_ERR_TIMEOUT, LU_ERR_UNSUPPORTED, LU_IR_CLASSIC, LU_IR_GMRES, LU_OK,
-                   LU_PREC_BF16, LU_PREC_FP16S, LU_PREC_FP16X3, LU_PREC_FP64)
+                   LU_PREC_BF16, LU_PREC_FP16S, LU_PREC_FP16X3, LU_PREC_FP32, LU_PREC_FP64)
 
 __all__ = ["LUConfig", "LUSolver", "LUError", "generate_uniform", "matgen", "status_string",
-           "LU_PREC_FP64", "LU_PREC_BF16", "LU_PREC_FP16S", "LU_PREC_FP16X3", "LU_IR_CLASSIC", "LU_IR_GMRES"]
+           "LU_PREC_FP64", "LU_PREC_BF16", "LU_PREC_FP16S", "LU_PREC_FP16X3", "LU_PREC_FP32", "LU_IR_CLASSIC", "LU_IR_GMRES"]
 
 EPS = 2.220446049250313e-16
 

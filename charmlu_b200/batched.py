@@ -1,0 +1,91 @@
+"""Batched uneven solves (no reference counterpart): many independent
+systems of different order factored and solved in one persistent launch
+(lu_batched_factor_solve).  Per-size-bucket kernel parameters come from the
+autotuner's tables in charmlu_b200/tuning/ when present."""
+import ctypes
+import json
+import os
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import LU_PREC_FP32, LU_PREC_FP64
+
+TUNING_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning")
+_applied = {}
+
+
+def tuning_path(precision):
+    return os.path.join(TUNING_DIR, "batched_fp64.json" if precision == LU_PREC_FP64 else "batched_fp32.json")
+
+
+def apply_tuning(precision, table=None):
+    """Load the autotuned {n_max, nb, small} table for this precision (or the
+    given table; [] restores the built-in defaults) into the kernel."""
+    L = _lib.load()
+    if table is None:
+        p = tuning_path(precision)
+        table = json.load(open(p))["table"] if os.path.exists(p) else []
+    flat = np.asarray([v for e in table for v in (e["n_max"], e["nb"], e["small"])], dtype=np.int32)
+    rc = L.lu_batched_set_tuning(len(table), ctypes.c_void_p(flat.ctypes.data) if len(table) else None)
+    if rc != 0:
+        raise RuntimeError(f"lu_batched_set_tuning failed ({rc})")
+    _applied["precision"] = precision
+
+
+class BatchedSystems:
+    """Device storage for `count` systems of orders n (host int array):
+    matrices concatenated row-major, right-hand sides concatenated."""
+
+    def __init__(self, n, device="cuda"):
+        self.n = np.asarray(n, dtype=np.int32)
+        self.count = len(self.n)
+        n64 = self.n.astype(np.int64)
+        self.a_off = np.concatenate([[0], np.cumsum(n64 * n64)[:-1]]).astype(np.int64)
+        self.b_off = np.concatenate([[0], np.cumsum(n64)[:-1]]).astype(np.int64)
+        self.total_a = int((n64 * n64).sum())
+        self.total_b = int(n64.sum())
+        self.d_n = torch.from_numpy(self.n).to(device)
+        self.d_a_off = torch.from_numpy(self.a_off).to(device)
+        self.d_b_off = torch.from_numpy(self.b_off).to(device)
+        self.info = torch.zeros(self.count, dtype=torch.int32, device=device)
+        self._work = {}
+
+    def work(self, precision):
+        if precision not in self._work:
+            L = _lib.load()
+            wb = L.lu_batched_work_bytes(self.count, ctypes.c_void_p(self.n.ctypes.data), precision)
+            self._work[precision] = torch.empty(wb, dtype=torch.uint8, device=self.d_n.device)
+        return self._work[precision]
+
+    def factor_solve(self, A, b, precision=LU_PREC_FP64, stream=None):
+        """A (total_a doubles), b (total_b doubles) on the device; b is
+        overwritten by the solutions, A by the factors (FP64) or left intact
+        (FP32 mode).  Returns the per-system status tensor (device)."""
+        if _applied.get("precision") != precision:
+            apply_tuning(precision)
+        L = _lib.load()
+        w = self.work(precision)
+        s = stream if stream is not None else torch.cuda.current_stream()
+        rc = L.lu_batched_factor_solve(self.count, ctypes.c_void_p(self.d_n.data_ptr()),
+                                       ctypes.c_void_p(self.d_a_off.data_ptr()),
+                                       ctypes.c_void_p(self.d_b_off.data_ptr()), ctypes.c_void_p(A.data_ptr()),
+                                       ctypes.c_void_p(b.data_ptr()), ctypes.c_void_p(self.info.data_ptr()),
+                                       precision, ctypes.c_void_p(w.data_ptr()), w.numel(),
+                                       ctypes.c_void_p(s.cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"lu_batched_factor_solve failed ({rc})")
+        return self.info
+
+
+def log_uniform_orders(count, lo=32, hi=1024, seed=42):
+    """Orders drawn log-uniform in [lo, hi] from the seed."""
+    rng = np.random.default_rng(seed)
+    n = np.exp(rng.uniform(np.log(lo), np.log(hi + 1), count)).astype(np.int32)
+    return np.clip(n, lo, hi)
+
+
+def flops(n):
+    n = np.asarray(n, dtype=np.float64)
+    return float((2.0 / 3.0 * n ** 3 + 2.0 * n ** 2).sum())

@@ -26,7 +26,7 @@
 //
 // LU_PREC_FP32: the FP32 copy of each matrix (workspace) is factored, then
 // FP64 refinement (r = b - A x against the FP64 A, FP32 correction solve,
-// FP64 update) until the system's scaled residual r_hpl < 16, at most 4
+// FP64 update) until the system's scaled residual r_hpl < 16, at most 10
 // steps.  One step is not enough at these orders: after one step r_hpl is
 // ~1e4 for a uniform n = 109 system (the remaining error lies along the
 // small singular directions); two steps bring it to O(1).
@@ -42,7 +42,7 @@ constexpr int BT = 512;                    // threads per CTA
 constexpr int NWARP = BT / 32;
 constexpr int kBatchMaxN = 2048;
 constexpr size_t kBatchSmem = 200 * 1024;  // dynamic shared memory per CTA
-constexpr int kBatchRefineMax = 4;         // FP64 refinement steps at most (FP32 mode)
+constexpr int kBatchRefineMax = 10;        // FP64 refinement steps at most (FP32 mode)
 
 struct Tuning {
   int n_max, nb, small;
@@ -292,8 +292,11 @@ __device__ int factor_system(T* A, int n, T* x, int* piv, unsigned char* smem, T
         if (i < kw) A[(int64_t)(k0 + i) * n + c] = u[i];
     }
     __syncthreads();
-    // trailing update A[c1:n, c1:n] -= L21 * U12 in 64 x 128 tiles, 4 x 4 per thread
-    const int tr = tid >> 5, tc = tid & 31;  // 16 row groups x 32 column groups
+    // trailing update A[c1:n, c1:n] -= L21 * U12 in 64 x 128 tiles, 4 x 4 per
+    // thread: rows tr*4 .. +3 (one row group per warp: the L21 reads are
+    // broadcasts), columns tc + 32 j (consecutive across lanes: conflict-free
+    // shared reads and coalesced global read-modify-writes)
+    const int tr = tid >> 5, tc = tid & 31;
     for (int ct = c1; ct < n; ct += 128) {
       for (int idx = tid; idx < kw * 128; idx += BT) {
         const int p = idx >> 7, c = idx & 127;
@@ -301,22 +304,26 @@ __device__ int factor_system(T* A, int n, T* x, int* piv, unsigned char* smem, T
       }
       __syncthreads();
       for (int rt = c1; rt < n; rt += 64) {
+        // C values first (their latency overlaps the FMA loop), then C -= L21 U12
+        const int rbase = rt + tr * 4;
         T acc[4][4];
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
-          for (int j = 0; j < 4; j++) acc[i][j] = 0;
-        const int rbase = rt + tr * 4;
+          for (int j = 0; j < 4; j++) {
+            const int r = rbase + i, c = ct + tc + 32 * j;
+            acc[i][j] = (r < n && c < n) ? A[(int64_t)r * n + c] : T(0);
+          }
         for (int p = 0; p < kw; p++) {
           T av[4], bv[4];
 #pragma unroll
           for (int i = 0; i < 4; i++) av[i] = (rbase + i < n) ? panel[(rbase + i - k0) * ld + p] : T(0);
 #pragma unroll
-          for (int j = 0; j < 4; j++) bv[j] = ut[p * 128 + tc * 4 + j];
+          for (int j = 0; j < 4; j++) bv[j] = ut[p * 128 + tc + 32 * j];
 #pragma unroll
           for (int i = 0; i < 4; i++)
 #pragma unroll
-            for (int j = 0; j < 4; j++) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+            for (int j = 0; j < 4; j++) acc[i][j] = fma(-av[i], bv[j], acc[i][j]);
         }
 #pragma unroll
         for (int i = 0; i < 4; i++) {
@@ -324,8 +331,8 @@ __device__ int factor_system(T* A, int n, T* x, int* piv, unsigned char* smem, T
           if (r >= n) break;
 #pragma unroll
           for (int j = 0; j < 4; j++) {
-            const int c = ct + tc * 4 + j;
-            if (c < n) A[(int64_t)r * n + c] -= acc[i][j];
+            const int c = ct + tc + 32 * j;
+            if (c < n) A[(int64_t)r * n + c] = acc[i][j];
           }
         }
       }

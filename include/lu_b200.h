@@ -173,7 +173,7 @@ LU_API int lu_adjoint(lu_handle h, const double* dLU, int64_t lda, const int32_t
  * and right-hand side at db + b_off[i] (overwritten by x).  precision:
  *   LU_PREC_FP64  FP64 factors in place in dA (as lu_factor);
  *   LU_PREC_FP32  FP32 factors of a copy in dWork, then FP64 refinement
- *                 against the untouched FP64 A until r_hpl < 16 (at most 4
+ *                 against the untouched FP64 A until r_hpl < 16 (at most 10
  *                 steps; LU_ERR_NOCONV in info[i] otherwise).
  * info[i] receives each system's status (0 or 1-based singular column).
  * dWork: device scratch of lu_batched_work_bytes(...) bytes.  All pointer
