@@ -18,6 +18,8 @@ Charm++ runtime) on the host cores, rank 0 only.
 """
 import argparse
 import json
+
+import numpy as np
 import os
 import subprocess
 import sys
@@ -245,6 +247,59 @@ def run_batched(args, rank, world):
     return 0
 
 
+def kappa_matrix(n, kappa, seed, dev):
+    """A = Q1 diag(sigma) Q2^T, Q from QR of seeded Gaussian matrices, sigma
+    geometric from 1 to 1/kappa (generated with torch on the GPU: input
+    construction only)."""
+    import torch
+    g = torch.Generator(device=dev).manual_seed(seed)
+    Q1, _ = torch.linalg.qr(torch.randn(n, n, dtype=torch.float64, device=dev, generator=g))
+    Q2, _ = torch.linalg.qr(torch.randn(n, n, dtype=torch.float64, device=dev, generator=g))
+    sig = torch.logspace(0, -float(np.log10(kappa)), n, dtype=torch.float64, device=dev)
+    return ((Q1 * sig) @ Q2.T).contiguous()
+
+
+def run_ksweep(args, rank, world):
+    """kappa sweep of the mixed path (BASELINE config 3 side sweep)."""
+    import scipy.linalg as sl
+    import torch
+    import charmlu_b200 as lu
+    if rank != 0:
+        return 0
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    n = args.ksweep_n
+    rows = []
+    precs = [("bf16", lu.LU_PREC_BF16), ("fp16s", lu.LU_PREC_FP16S), ("fp16x3", lu.LU_PREC_FP16X3)]
+    for kappa in (1e2, 1e6, 1e10):
+        A = kappa_matrix(n, kappa, 1234, dev)
+        b = lu.generate_uniform(n, 1, seed=42, stream_id=1, device=dev).view(-1)
+        x_ref = sl.solve(A.cpu().numpy(), b.cpu().numpy(), check_finite=False)  # FP64 LAPACK oracle solution
+        for name, prec in precs:
+            s = lu.LUSolver(lu.LUConfig(n, 512, precision=prec, ir_max_iter=args.ksweep_iters))
+            x = torch.empty_like(b)
+            s.refine_solve(A, b, x)  # warm (allocations)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _, info = s.refine_solve(A, b, x)
+            e1.record()
+            torch.cuda.synchronize()
+            st = s.status()
+            r = s.residual(A, x, b)
+            fe = float(np.abs(x.cpu().numpy() - x_ref).max() / np.abs(x_ref).max())
+            rows.append({"kappa": kappa, "precision": name, "status": st, "converged": st == 0,
+                         "ir_iterations": info["iterations"], "gmres_iterations": info["gmres_iterations"],
+                         "used_gmres": bool(info["used_gmres"]), "r_hpl": r["r_hpl"],
+                         "r_hpl_initial": info["r_hpl_initial"], "forward_error_vs_fp64": fe,
+                         "kappa_eps": kappa * 2.22e-16, "ms": e0.elapsed_time(e1)})
+            print(json.dumps(rows[-1]), flush=True)
+            del s
+        del A
+        torch.cuda.empty_cache()
+    print(json.dumps({"metric": f"kappa sweep N={n}", "rows": rows}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -261,7 +316,9 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=8192)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="lu", choices=["lu", "batched"])
+    ap.add_argument("--workload", default="lu", choices=["lu", "batched", "ksweep"])
+    ap.add_argument("--ksweep-n", type=int, default=8192)
+    ap.add_argument("--ksweep-iters", type=int, default=30)
     ap.add_argument("--batch-count", type=int, default=4096)
     args = ap.parse_args()
 
@@ -272,6 +329,8 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "batched":
         return run_batched(args, rank, world)
+    if args.workload == "ksweep":
+        return run_ksweep(args, rank, world)
 
     import torch
     import charmlu_b200 as lu

@@ -124,6 +124,12 @@ __global__ void gather_f64_to_f32_kernel(const double* __restrict__ v, const int
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) y[i] = (float)(v[perm[i]] * scale);
 }
+__global__ void gather_f64_kernel(const double* __restrict__ v, const int32_t* __restrict__ perm,
+                                  double* __restrict__ y, int n, double scale, const ResidualAccum* acc) {
+  const double sc = acc ? 1.0 / rnorm_of(acc) : scale;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = v[perm[i]] * sc;
+}
 __global__ void f32_to_f64_kernel(const float* __restrict__ y, double* __restrict__ x, int n, double scale) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) x[i] = (double)y[i] * scale;
@@ -151,8 +157,7 @@ __global__ void __launch_bounds__(256) multi_dot_part_kernel(const double* __res
   }
 }
 __global__ void multi_dot_final_kernel(const double* __restrict__ part, int k, double* __restrict__ out) {
-  const int j = threadIdx.x;
-  if (j < k) {
+  for (int j = threadIdx.x; j < k; j += blockDim.x) {
     double t = 0.0;
     for (int b = 0; b < kDotBlocks; b++) t += part[j * kDotBlocks + b];
     out[j] = t;
@@ -182,7 +187,7 @@ int launch_multi_dot(const double* V, int k, const double* w, int n, double* par
   if (k <= 0) return LU_OK;
   multi_dot_part_kernel<<<dim3(kDotBlocks, k), 256, 0, s>>>(V, w, n, part);
   LUB_LAUNCH_CHECK();
-  multi_dot_final_kernel<<<1, 64, 0, s>>>(part, k, out);
+  multi_dot_final_kernel<<<1, 256, 0, s>>>(part, k, out);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }
@@ -258,6 +263,12 @@ int launch_ir_update(double* x, const float* d32, int n, const ResidualAccum* ac
 }
 int launch_gather_f64_to_f32(const double* v, const int32_t* perm, float* y, int n, double scale, cudaStream_t s) {
   gather_f64_to_f32_kernel<<<ceil_div(n, 256), 256, 0, s>>>(v, perm, y, n, scale);
+  LUB_LAUNCH_CHECK();
+  return LU_OK;
+}
+int launch_gather_f64(const double* v, const int32_t* perm, double* y, int n, double scale, const ResidualAccum* acc,
+                      cudaStream_t s) {
+  gather_f64_kernel<<<ceil_div(n, 256), 256, 0, s>>>(v, perm, y, n, scale, acc);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }

@@ -86,6 +86,14 @@ struct ResidualAccum {  // non-negative doubles stored as ordered bit patterns
 };
 int launch_residual_f64(const double* A, int64_t lda, int n, const double* x, const double* b, double* r,
                         ResidualAccum* acc, cudaStream_t s);
+// factors stored as TS, vector and arithmetic in T (FP32 factors, FP64 vector)
+template <typename TS, typename T>
+int launch_trsv_mixed(const TS* LU, int64_t lda, int n, T* x, int upper, int* flags, unsigned* ticket, DevStatus* st,
+                      long long spin, cudaStream_t s);
+// y[i] = v[perm[i]] * scale (scale = 1/||r||inf from acc when acc is given)
+int launch_gather_f64(const double* v, const int32_t* perm, double* y, int n, double scale, const ResidualAccum* acc,
+                      cudaStream_t s);
+
 int launch_gen_uniform(double* d, int64_t rows, int64_t cols, int64_t ld, uint64_t seed, uint64_t stream_id,
                        cudaStream_t s);
 int launch_gather_perm(const double* b, const int32_t* perm, double* y, int n, cudaStream_t s);

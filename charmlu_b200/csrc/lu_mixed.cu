@@ -22,7 +22,7 @@ using namespace lub;
 
 namespace {
 
-constexpr int kGmresRestart = 30;
+constexpr int kGmresRestart = 120;  // long Krylov spaces: short restarts stall when kappa * u_f >> 1
 
 int ensure_mixed(lu_handle h) {
   if (h->mixed_ready) return LU_OK;
@@ -42,7 +42,7 @@ int ensure_mixed(lu_handle h) {
   LUB_TRY(h->alloc(&h->z64, n));
   LUB_TRY(h->alloc(&h->zero64, n));
   LUB_TRY(h->alloc(&h->V, (size_t)(h->gm + 1) * n));
-  LUB_TRY(h->alloc(&h->hdot, 128 * 64 + 64));
+  LUB_TRY(h->alloc(&h->hdot, 128 * (h->gm + 2) + 2 * (h->gm + 2)));
   LUB_CUDA(cudaMemset(h->zero64, 0, sizeof(double) * n));
   h->mixed_ready = true;
   return LU_OK;
@@ -209,6 +209,16 @@ int solve32(lu_handle h, float* v, cudaStream_t s) {
   return launch_trsv<float>(h->A32, h->ld32, n, v, 1, h->trsv_flags, h->trsv_ticket, h->st, h->spin, s);
 }
 
+// M^{-1} v in working precision: FP32 factors, FP64 vector and arithmetic
+int solve_f32_factors_f64(lu_handle h, double* v, cudaStream_t s) {
+  const int n = (int)h->cfg.n;
+  Prof pf(h, s, LU_PH_SOLVE, 2.0 * n * (double)n);
+  LUB_TRY((launch_trsv_mixed<float, double>(h->A32, h->ld32, n, v, 0, h->trsv_flags, h->trsv_ticket, h->st,
+                                             h->spin, s)));
+  return launch_trsv_mixed<float, double>(h->A32, h->ld32, n, v, 1, h->trsv_flags, h->trsv_ticket, h->st, h->spin,
+                                           s);
+}
+
 double bits_to_double(unsigned long long v) {
   double x;
   memcpy(&x, &v, 8);
@@ -241,9 +251,9 @@ int device_status(lu_handle h, cudaStream_t s) {
   return st.code != 0 ? st.code : st.info;
 }
 
-// Right-preconditioned-equivalent left-preconditioned GMRES on the
-// correction: M^{-1} A d = M^{-1} r with M = P^T L U (FP32 factors), FP64
-// Arnoldi with two passes of classical Gram-Schmidt.  x += d.
+// Left-preconditioned GMRES on the correction: M^{-1} A d = M^{-1} r with
+// M = P^T L U (FP32 factors applied in FP64), FP64 Arnoldi with two passes of
+// classical Gram-Schmidt.  x += d.
 // rnorm: ||r||inf of the residual in h->r64 (the start vector is built from
 // r / rnorm, so the Krylov right-hand side is beta * rnorm).
 int gmres_correction(lu_handle h, const double* A, int64_t lda, double* x, double rnorm, cudaStream_t s,
@@ -251,12 +261,13 @@ int gmres_correction(lu_handle h, const double* A, int64_t lda, double* x, doubl
   const int n = (int)h->cfg.n, m = h->gm;
   double* V = h->V;
   double* part = h->hdot;
-  double* hd = h->hdot + 128 * 64;  // 64 doubles of results
+  double* hd = h->hdot + 128 * (m + 2);  // m + 2 doubles of results
   std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1, 0.0), hcol(m + 1);
-  // v0 = M^{-1} r / ||M^{-1} r||  (r already in h->r64, racc holds ||r||)
-  LUB_TRY(launch_ir_prep(h->r64, h->perm, h->v32, n, h->racc, s));
-  LUB_TRY(solve32(h, h->v32, s));
-  LUB_TRY(launch_f32_to_f64(h->v32, V, n, 1.0, s));
+  // v0 = M^{-1} r / ||M^{-1} r||  (r already in h->r64, racc holds ||r||);
+  // the preconditioner is applied in working precision (FP64 vectors and
+  // arithmetic on the FP32 factors), which GMRES-IR's convergence needs
+  LUB_TRY(launch_gather_f64(h->r64, h->perm, V, n, 1.0, h->racc, s));
+  LUB_TRY(solve_f32_factors_f64(h, V, s));
   LUB_TRY(launch_multi_dot(V, 1, V, n, part, hd, s));
   double beta2 = 0.0;
   LUB_CUDA(cudaMemcpyAsync(&beta2, hd, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -274,9 +285,8 @@ int gmres_correction(lu_handle h, const double* A, int64_t lda, double* x, doubl
       Prof pf(h, s, LU_PH_OTHER);
       LUB_TRY(launch_residual_f64(A, lda, n, vj, h->zero64, h->z64, h->racc, s));
     }
-    LUB_TRY(launch_gather_f64_to_f32(h->z64, h->perm, h->v32, n, -1.0, s));
-    LUB_TRY(solve32(h, h->v32, s));
-    LUB_TRY(launch_f32_to_f64(h->v32, w, n, 1.0, s));
+    LUB_TRY(launch_gather_f64(h->z64, h->perm, w, n, -1.0, nullptr, s));
+    LUB_TRY(solve_f32_factors_f64(h, w, s));
     // two passes of classical Gram-Schmidt
     std::fill(hcol.begin(), hcol.end(), 0.0);
     for (int pass = 0; pass < 2; pass++) {
@@ -350,13 +360,17 @@ int refine_solve(lu_handle h, const double* A, int64_t lda, const double* b, dou
   const int max_it = h->cfg.ir_max_iter > 0 ? h->cfg.ir_max_iter : 50;
   bool gm = h->cfg.ir_mode == LU_IR_GMRES;
   double prev = INFINITY, r_hpl = INFINITY, rn = 0.0;
-  int it = 0;
+  int it = 0, gm_stall = 0;
   for (; it < max_it; it++) {
     LUB_TRY(residual_hpl(h, A, lda, x, b, h->r64, &r_hpl, &rn, s));
     if (it == 0) ri.r_hpl_initial = r_hpl;
     if (!std::isfinite(r_hpl)) break;
     if (r_hpl < target) break;
     if (!gm && it >= 2 && r_hpl > 0.5 * prev) gm = true;  // classical IR stopped contracting
+    // GMRES cycles that no longer reduce the residual: the low-precision
+    // factors have lost too much of A's spectrum; report non-convergence
+    if (ri.used_gmres) gm_stall = (r_hpl > 0.9 * prev) ? gm_stall + 1 : 0;
+    if (gm_stall >= 3) break;
     prev = r_hpl;
     if (gm) {
       int k = 0;

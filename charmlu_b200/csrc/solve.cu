@@ -46,8 +46,11 @@ __global__ void __launch_bounds__(128) trsm_llu_leaf_kernel(const T* L, int64_t 
 
 constexpr int TB = 64;  // rows per TRSV block
 
-template <typename T, bool UPPER>
-__global__ void __launch_bounds__(256) trsv_kernel(const T* LU, int64_t lda, int n, T* x, int* flags,
+// TS: storage type of the factors; T: type of the vector and the arithmetic
+// (FP32 factors with an FP64 vector give the GMRES-IR preconditioner solve
+// in working precision at the FP32 factors' memory cost).
+template <typename TS, typename T, bool UPPER>
+__global__ void __launch_bounds__(256) trsv_kernel(const TS* LU, int64_t lda, int n, T* x, int* flags,
                                                    unsigned* ticket, DevStatus* st, long long spin) {
   __shared__ T sD[TB][TB + 1];
   __shared__ T s_acc[TB];
@@ -63,7 +66,7 @@ __global__ void __launch_bounds__(256) trsv_kernel(const T* LU, int64_t lda, int
 
   for (int idx = tid; idx < TB * TB; idx += blockDim.x) {
     const int i = idx / TB, j = idx - i * TB;
-    sD[i][j] = (i < rows && j < rows) ? LU[(int64_t)(r0 + i) * lda + r0 + j] : T(0);
+    sD[i][j] = (i < rows && j < rows) ? (T)LU[(int64_t)(r0 + i) * lda + r0 + j] : T(0);
   }
 
   T acc[8];
@@ -81,7 +84,7 @@ __global__ void __launch_bounds__(256) trsv_kernel(const T* LU, int64_t lda, int
 #pragma unroll
       for (int e = 0; e < 2; e++) {
         const int c = c0 + lane * 2 + e;
-        lv[i][e] = (r < n && c < n) ? __ldcs(&LU[(int64_t)r * lda + c]) : T(0);
+        lv[i][e] = (r < n && c < n) ? (T)__ldcs(&LU[(int64_t)r * lda + c]) : T(0);
       }
     }
     if (lane == 0) {
@@ -345,20 +348,28 @@ int launch_trsm_llu_leaf(const T* L, int64_t ldl, T* B, int64_t ldb, int m, int 
   return LU_OK;
 }
 
-template <typename T>
-int launch_trsv(const T* LU, int64_t lda, int n, T* x, int upper, int* flags, unsigned* ticket, DevStatus* st,
-                long long spin, cudaStream_t s) {
+template <typename TS, typename T>
+int launch_trsv_mixed(const TS* LU, int64_t lda, int n, T* x, int upper, int* flags, unsigned* ticket, DevStatus* st,
+                      long long spin, cudaStream_t s) {
   if (n <= 0) return LU_OK;
   const int nblk = ceil_div(n, TB);
   LUB_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * nblk, s));
   LUB_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), s));
   if (upper)
-    trsv_kernel<T, true><<<nblk, 256, 0, s>>>(LU, lda, n, x, flags, ticket, st, spin);
+    trsv_kernel<TS, T, true><<<nblk, 256, 0, s>>>(LU, lda, n, x, flags, ticket, st, spin);
   else
-    trsv_kernel<T, false><<<nblk, 256, 0, s>>>(LU, lda, n, x, flags, ticket, st, spin);
+    trsv_kernel<TS, T, false><<<nblk, 256, 0, s>>>(LU, lda, n, x, flags, ticket, st, spin);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }
+
+template <typename T>
+int launch_trsv(const T* LU, int64_t lda, int n, T* x, int upper, int* flags, unsigned* ticket, DevStatus* st,
+                long long spin, cudaStream_t s) {
+  return launch_trsv_mixed<T, T>(LU, lda, n, x, upper, flags, ticket, st, spin, s);
+}
+template int launch_trsv_mixed<float, double>(const float*, int64_t, int, double*, int, int*, unsigned*, DevStatus*,
+                                              long long, cudaStream_t);
 
 template int launch_trsm_llu_leaf<double>(const double*, int64_t, double*, int64_t, int, int, cudaStream_t);
 template int launch_trsm_llu_leaf<float>(const float*, int64_t, float*, int64_t, int, int, cudaStream_t);

@@ -141,3 +141,35 @@ def test_refine_lookahead(cuda_dev, n, b):
     s, A, rhs, x, info, st = _refine(n, b, lookahead=True)
     assert st == 0 and info["status"] == 0, info
     assert s.residual(A, x, rhs)["r_hpl"] < 16
+
+
+@pytest.mark.parametrize("kappa", [1e2, 1e6])
+def test_kappa_matrices_refine_or_report(cuda_dev, kappa):
+    """Q1 diag(sigma) Q2^T test matrices: a refined result either meets the
+    residual contract (checked independently here) or is reported as not
+    converged; never a silent wrong answer."""
+    import sys, os
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from bench import kappa_matrix
+    import charmlu_b200 as lu
+    n = 1024
+    A = kappa_matrix(n, kappa, 99, torch.device("cuda"))
+    b = lu.generate_uniform(n, 1, seed=42, stream_id=1).view(-1)
+    x_ref = np.linalg.solve(A.cpu().numpy(), b.cpu().numpy())
+    for prec in (lu.LU_PREC_FP16S, lu.LU_PREC_FP16X3):
+        s = lu.LUSolver(lu.LUConfig(n, 256, precision=prec, ir_max_iter=30))
+        x, info = s.refine_solve(A, b)
+        st = s.status()
+        r = s.residual(A, x, b)
+        if st == 0:
+            assert r["r_hpl"] < 16, (prec, r)
+            fe = np.abs(x.cpu().numpy() - x_ref).max() / np.abs(x_ref).max()
+            # backward error ~ r_hpl * n * eps, forward error <~ kappa * that
+            assert fe < 4 * kappa * max(r["r_hpl"], 1.0) * n * 2.2e-16, (prec, fe)
+        else:
+            assert st == lu.LU_ERR_NOCONV
+    # the error-compensated factors converge classically at kappa = 1e2
+    if kappa == 1e2:
+        s = lu.LUSolver(lu.LUConfig(n, 256, precision=lu.LU_PREC_FP16X3))
+        x, info = s.refine_solve(A, b)
+        assert s.status() == 0 and info["used_gmres"] == 0
