@@ -79,6 +79,19 @@ struct lu_handle_s {
   std::vector<void*> allocs;
   size_t bytes = 0;
   long long spin = 0;
+  // CUDA-graph replay of factorisation schedules (cfg.use_graph)
+  struct GraphSlot {
+    const void* k1 = nullptr;
+    const void* k2 = nullptr;
+    const void* k3 = nullptr;
+    int64_t k4 = 0;
+    cudaGraphExec_t exec = nullptr;
+    long long kernels = 0;  // kernel nodes per replay (added to the launch count)
+  };
+  GraphSlot gslot[2];            // 0: FP64 factor, 1: mixed factor
+  cudaStream_t sG = nullptr;     // capture / replay stream
+  cudaEvent_t evG0 = nullptr, evG1 = nullptr;
+  bool capturing = false;
   // phase profiling (events on the launching stream)
   int profile = 0;
   struct Rec {
@@ -127,18 +140,72 @@ struct Prof {
   double fl;
   cudaEvent_t a = nullptr;
   Prof(lu_handle h_, cudaStream_t s_, int ph_, double fl_ = 0.0) : h(h_), s(s_), ph(ph_), fl(fl_) {
-    if (h->profile) {
+    if (h->profile && !h->capturing) {
       a = h->take_event();
       cudaEventRecord(a, s);
     }
   }
   ~Prof() {
-    if (h->profile) {
+    if (a) {
       cudaEvent_t b = h->take_event();
       cudaEventRecord(b, s);
       h->recs.push_back({ph, a, b, fl});
     }
   }
 };
+
+// Run body(stream) as a CUDA graph keyed by (k1..k4): replay the cached graph
+// when the keys match, otherwise capture body on the handle's capture stream
+// (forked from and joined back to s by events), instantiate and launch.
+// Without use_graph, body runs directly on s.
+template <typename F>
+int run_graph(lu_handle h, int slot, const void* k1, const void* k2, const void* k3, int64_t k4, cudaStream_t s,
+              F&& body) {
+  if (!h->cfg.use_graph) return body(s);
+  auto& g = h->gslot[slot];
+  LUB_CUDA(cudaEventRecord(h->evG0, s));
+  LUB_CUDA(cudaStreamWaitEvent(h->sG, h->evG0, 0));
+  if (!(g.exec && g.k1 == k1 && g.k2 == k2 && g.k3 == k3 && g.k4 == k4)) {
+    if (g.exec) {
+      cudaGraphExecDestroy(g.exec);
+      g.exec = nullptr;
+    }
+    LUB_CUDA(cudaStreamBeginCapture(h->sG, cudaStreamCaptureModeThreadLocal));
+    h->capturing = true;
+    const long long before = __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED);
+    const int rc = body(h->sG);
+    // captured, not launched: the replays below count them
+    __atomic_store_n(&g_kernel_launches, before, __ATOMIC_RELAXED);
+    h->capturing = false;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->sG, &graph);
+    if (rc != LU_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    LUB_CUDA(e);
+    size_t nn = 0;
+    cudaGraphGetNodes(graph, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (nn) cudaGraphGetNodes(graph, nodes.data(), &nn);
+    g.kernels = 0;
+    for (auto nd : nodes) {
+      cudaGraphNodeType t;
+      if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) g.kernels++;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    LUB_CUDA(ei);
+    g.k1 = k1;
+    g.k2 = k2;
+    g.k3 = k3;
+    g.k4 = k4;
+  }
+  LUB_CUDA(cudaGraphLaunch(g.exec, h->sG));
+  __atomic_add_fetch(&g_kernel_launches, g.kernels, __ATOMIC_RELAXED);
+  LUB_CUDA(cudaEventRecord(h->evG1, h->sG));
+  LUB_CUDA(cudaStreamWaitEvent(s, h->evG1, 0));
+  return LU_OK;
+}
 
 }  // namespace lub

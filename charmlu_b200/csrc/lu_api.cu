@@ -161,9 +161,16 @@ int check_common(lu_handle h, const void* dA, int64_t lda) {
   return ensure_kernels_init();
 }
 
+int factor_f64_schedule(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double* rhs, cudaStream_t s);
+
 int factor_f64(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double* rhs, cudaStream_t s) {
   LUB_TRY(check_common(h, dA, lda));
   if (!ipiv) return LU_ERR_ARG;
+  return run_graph(h, 0, dA, ipiv, rhs, lda, s,
+                   [&](cudaStream_t ss) { return factor_f64_schedule(h, dA, lda, ipiv, rhs, ss); });
+}
+
+int factor_f64_schedule(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double* rhs, cudaStream_t s) {
   const int n = (int)h->cfg.n, b = h->cfg.block_size;
   const bool la = h->cfg.lookahead != 0;
   Ctx64 c;
@@ -300,7 +307,10 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
     if (cudaStreamCreateWithPriority(&h->sP, cudaStreamNonBlocking, hi) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->evP, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->evN, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&h->evN, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->sG, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->evG0, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->evG1, cudaEventDisableTiming) != cudaSuccess)
       s = LU_ERR_CUDA;
   }
   h->leaf_ctas = h->num_sms;
@@ -334,6 +344,11 @@ int lu_destroy(lu_handle h) {
   if (h->evP) cudaEventDestroy(h->evP);
   if (h->evN) cudaEventDestroy(h->evN);
   if (h->sP) cudaStreamDestroy(h->sP);
+  for (auto& g : h->gslot)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (h->evG0) cudaEventDestroy(h->evG0);
+  if (h->evG1) cudaEventDestroy(h->evG1);
+  if (h->sG) cudaStreamDestroy(h->sG);
   for (void* p : h->allocs) cudaFree(p);
   if (h->racc_host) cudaFreeHost(h->racc_host);
   delete h;

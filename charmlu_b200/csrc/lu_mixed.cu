@@ -339,11 +339,13 @@ int refine_solve(lu_handle h, const double* A, int64_t lda, const double* b, dou
   const int n = (int)h->cfg.n;
   LUB_TRY(ensure_mixed(h));
   LUB_CUDA(cudaMemsetAsync(h->st, 0, sizeof(DevStatus), s));
-  {
-    Prof pf(h, s, LU_PH_OTHER);
-    LUB_TRY(launch_f64_to_f32(A, lda, h->A32, h->ld32, n, n, s));
-  }
-  LUB_TRY(factor_mixed(h, s));
+  LUB_TRY(run_graph(h, 1, A, h->A32, nullptr, lda, s, [&](cudaStream_t ss) {
+    {
+      Prof pf(h, ss, LU_PH_OTHER);
+      LUB_TRY(launch_f64_to_f32(A, lda, h->A32, h->ld32, n, n, ss));
+    }
+    return factor_mixed(h, ss);
+  }));
   // x0 = U^{-1} L^{-1} P b in FP32
   LUB_TRY(launch_gather_f64_to_f32(b, h->perm, h->v32, n, 1.0, s));
   LUB_TRY(solve32(h, h->v32, s));

@@ -238,3 +238,27 @@ def test_lookahead_trailing_update_identical_to_serial(cuda_dev):
     assert torch.equal(p1, p2)
     # leaf widths differ between the schedules (32 vs 16), so only near-equality
     assert (A1 - A2).abs().max().item() <= 1e-12 * A1.abs().max().item()
+
+
+@pytest.mark.parametrize("lookahead", [False, True])
+def test_graph_replay_identical(cuda_dev, lookahead):
+    """use_graph: the schedule is captured once per buffer set and replayed;
+    replays give bit-identical factors, and new buffers trigger a new capture."""
+    import charmlu_b200 as lu
+    n, b = 1536, 128
+    A = oracle.gen_matrix(n, 41)
+    ref = lu.LUSolver(lu.LUConfig(n, b, lookahead=lookahead))
+    Ar = torch.from_numpy(A).cuda()
+    pr = ref.factor(Ar)
+    assert ref.status() == 0
+    g = lu.LUSolver(lu.LUConfig(n, b, lookahead=lookahead, use_graph=True))
+    Ad = torch.empty_like(Ar)
+    ip = torch.empty(n, dtype=torch.int32, device="cuda")
+    for _ in range(3):  # capture, then two replays on the same buffers
+        Ad.copy_(torch.from_numpy(A))
+        g.factor(Ad, ipiv=ip)
+        assert g.status() == 0
+        assert torch.equal(ip, pr) and torch.equal(Ad, Ar)
+    A2 = torch.from_numpy(A).cuda()  # different buffer: re-capture
+    p2 = g.factor(A2)
+    assert g.status() == 0 and torch.equal(A2, Ar) and torch.equal(p2, pr)

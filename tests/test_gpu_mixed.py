@@ -173,3 +173,18 @@ def test_kappa_matrices_refine_or_report(cuda_dev, kappa):
         s = lu.LUSolver(lu.LUConfig(n, 256, precision=lu.LU_PREC_FP16X3))
         x, info = s.refine_solve(A, b)
         assert s.status() == 0 and info["used_gmres"] == 0
+
+
+def test_refine_graph_replay(cuda_dev):
+    import charmlu_b200 as lu
+    n, b = 2048, 256
+    A = lu.generate_uniform(n, n, seed=42, stream_id=0)
+    rhs = lu.generate_uniform(n, 1, seed=42, stream_id=1).view(-1)
+    s0 = lu.LUSolver(lu.LUConfig(n, b, precision=lu.LU_PREC_FP16X3, lookahead=True))
+    x0, _ = s0.refine_solve(A, rhs)
+    sg = lu.LUSolver(lu.LUConfig(n, b, precision=lu.LU_PREC_FP16X3, lookahead=True, use_graph=True))
+    x = torch.empty_like(rhs)
+    for _ in range(3):
+        _, info = sg.refine_solve(A, rhs, x)
+        assert sg.status() == 0 and info["status"] == 0
+        assert torch.equal(x, x0)
