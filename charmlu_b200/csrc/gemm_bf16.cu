@@ -216,10 +216,190 @@ gemm_bf16_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_const
   }
 }
 
+// ---------------------------------------------------------------------------
+// Persistent variant: a fixed grid (the SM count, less any SMs left free for
+// a panel running beside it) walks the tiles in grouped-raster order.  TMEM
+// holds two 128 x 256 FP32 accumulators, so the epilogue of tile i (warps
+// 2-5, named barrier 1) overlaps the MMAs of tile i+1 (warp 1) while warp 0
+// keeps the TMA ring full across tile boundaries.
+//   barriers: full/empty[STAGES] (operand ring), tfull/tempty[2] (accumulator
+//   handoff; tempty counts the four epilogue warps)
+// ---------------------------------------------------------------------------
+constexpr int P_THREADS = 192;
+constexpr int P_TMEM_COLS = 512;
+
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+__global__ void __launch_bounds__(P_THREADS, 1)
+gemm_lowp_persistent_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                            const __grid_constant__ CUtensorMap mapC, Bf16GemmArgs args) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char* epi = smem + STAGES * STAGE_BYTES;
+  uint64_t* full = reinterpret_cast<uint64_t*>(epi + 2 * EPI_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* tfull = empty + STAGES;
+  uint64_t* tempty = tfull + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+  __shared__ int s_epi_fail;  // sticky: the epilogue warps stop together
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ntm = (args.M + BM - 1) / BM, ntn = (args.N + BN - 1) / BN;
+  const int tiles = ntm * ntn;
+  const int KT = (args.K + BK - 1) / BK;
+  const long long lim = args.spin >> 4;
+
+  if (tid == 0) {
+    prefetch_tmap(&mapA);
+    prefetch_tmap(&mapB);
+    prefetch_tmap(&mapC);
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);
+    }
+    fence_mbar_init();
+    s_epi_fail = 0;
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(P_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {  // ---- TMA producer
+      long long kb = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+        int tm, tn;
+        grouped_tile(t, ntm, ntn, 16, tm, tn);
+        for (int kt = 0; kt < KT; kt++, kb++) {
+          const int s = (int)(kb % STAGES);
+          if (kb >= STAGES && !mbar_wait(&empty[s], (uint32_t)(((kb / STAGES) - 1) & 1), args.st, lim, 411)) {
+            ok = false;
+            break;
+          }
+          unsigned char* sa = smem + s * STAGE_BYTES;
+          mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+          tma_load_2d(sa, &mapA, &full[s], kt * BK, args.a_row0 + tm * BM);
+          tma_load_2d(sa + A_BYTES, &mapB, &full[s], kt * BK, args.b_row0 + tn * BN);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // ---- MMA issuer
+      long long kb = 0;
+      int i = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, i++) {
+        const int ab = i & 1, u = i >> 1;
+        if (u >= 1 && !mbar_wait(&tempty[ab], (uint32_t)((u - 1) & 1), args.st, lim, 412)) break;
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(ab * 256);
+        for (int kt = 0; kt < KT; kt++, kb++) {
+          const int s = (int)(kb % STAGES);
+          if (!mbar_wait(&full[s], (uint32_t)((kb / STAGES) & 1), args.st, lim, 413)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a_addr = smem_u32(smem + s * STAGE_BYTES);
+          const uint32_t b_addr = a_addr + A_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; kk++)
+            umma_f16(d, smem_desc_k128(a_addr + kk * 32), smem_desc_k128(b_addr + kk * 32), args.idesc,
+                     (kt > 0 || kk > 0) ? 1u : 0u);
+          umma_commit(&empty[s]);
+        }
+        umma_commit(&tfull[ab]);
+      }
+    }
+  } else {
+    // ---- epilogue warps 2..5: a warp reads TMEM lanes 32 * (warp % 4) ..
+    const int q = warp & 3;
+    const int row = q * 32 + lane;
+    const bool leader = (warp == 2 && lane == 0);
+    // operands were scaled by powers of two; undo exactly on the accumulator
+    const float unscale = args.amax ? pow2_unscale(args.amax) : 1.f;
+    long long chunk = 0;
+    int i = 0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x, i++) {
+      int tm, tn;
+      grouped_tile(t, ntm, ntn, 16, tm, tn);
+      const int ab = i & 1, u = i >> 1;
+      if (!mbar_wait(&tfull[ab], (uint32_t)(u & 1), args.st, lim, 414) && lane == 0) atomicOr(&s_epi_fail, 1);
+      // agree across the four warps before the warp-collective loads
+      epi_bar();
+      const bool ok = *(volatile int*)&s_epi_fail == 0;
+      tc_fence_after();
+      for (int c = 0; c < BN / EPI_COLS; c++, chunk++) {
+        uint32_t v[32];
+        if (ok) tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * 256 + c * EPI_COLS), v);
+        if (c == BN / EPI_COLS - 1) {
+          // all of this accumulator has been read: hand it back to the MMA warp
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&tempty[ab]);
+        }
+        if (leader) bulk_wait_read<1>();  // the box written two chunks ago has been read
+        epi_bar();
+        unsigned char* box = epi + (int)(chunk & 1) * EPI_BYTES;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          float4 f = make_float4(-__uint_as_float(v[4 * j]) * unscale, -__uint_as_float(v[4 * j + 1]) * unscale,
+                                 -__uint_as_float(v[4 * j + 2]) * unscale, -__uint_as_float(v[4 * j + 3]) * unscale);
+          *reinterpret_cast<float4*>(box + row * 128 + ((j ^ (row & 7)) << 4)) = f;
+        }
+        fence_proxy_async();
+        epi_bar();
+        if (leader && ok) {
+          tma_reduce_add_2d(&mapC, box, args.c_col0 + tn * BN + c * EPI_COLS, args.c_row0 + tm * BM);
+          bulk_commit();
+        }
+      }
+      if (!ok) break;
+    }
+    if (leader) bulk_wait_all();
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P_TMEM_COLS) : "memory");
+  }
+}
+
 }  // namespace
 
 int gemm_bf16_init() {
   LUB_CUDA(cudaFuncSetAttribute(gemm_bf16_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+  LUB_CUDA(
+      cudaFuncSetAttribute(gemm_lowp_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+  return LU_OK;
+}
+
+// Persistent launch: grid = min(tiles, max_ctas).
+int launch_gemm_lowp_persistent(const CUtensorMap& mapA, const CUtensorMap& mapB, const CUtensorMap& mapC,
+                                int a_row0, int b_row0, int c_row0, int c_col0, int M, int N, int K, bool bf16,
+                                const unsigned* amax, DevStatus* st, long long spin, int max_ctas, cudaStream_t s) {
+  if (M <= 0 || N <= 0 || K <= 0) return LU_OK;
+  if (c_col0 & 3) return LU_ERR_ALIGN;
+  Bf16GemmArgs a{a_row0, b_row0, c_row0, c_col0, M, N, K, make_idesc(bf16), amax, st, spin};
+  const int64_t tiles = (int64_t)ceil_div(N, BN) * ceil_div(M, BM);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, std::max(1, max_ctas)));
+  gemm_lowp_persistent_kernel<<<grid, P_THREADS, SMEM_BYTES, s>>>(mapA, mapB, mapC, a);
+  LUB_LAUNCH_CHECK();
   return LU_OK;
 }
 
@@ -254,6 +434,10 @@ extern "C" __attribute__((visibility("default"))) int lub_test_gemm_lowp(const f
                                                                          int N, int K, int mode, void* stream) {
   using namespace lub;
   cudaStream_t s = (cudaStream_t)stream;
+  // mode bits 0-7: 0 bf16, 1 scaled fp16, 2 split fp16 x3; bits 8+: CTA count
+  // of the persistent kernel (0: one CTA per tile)
+  const int pctas = mode >> 8;
+  mode &= 0xff;
   if (M <= 0 || N <= 0 || K <= 0 || mode < 0 || mode > 2 || (ldc & 3) || (reinterpret_cast<uintptr_t>(C) & 15))
     return LU_ERR_ARG;
   LUB_TRY(gemm_bf16_init());
@@ -286,7 +470,10 @@ extern "C" __attribute__((visibility("default"))) int lub_test_gemm_lowp(const f
   if (rc == LU_OK) rc = encode_tmap_2d(&mU, dt, 2, Ub, Ke, N, ldk * 2, 64, 256, CU_TENSOR_MAP_SWIZZLE_128B);
   if (rc == LU_OK)
     rc = encode_tmap_2d(&mC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, N, M, ldc * 4, 32, 128, CU_TENSOR_MAP_SWIZZLE_128B);
-  if (rc == LU_OK)
+  if (rc == LU_OK && pctas > 0)
+    rc = launch_gemm_lowp_persistent(mL, mU, mC, 0, 0, 0, 0, M, N, Ke, bf16, bf16 ? nullptr : amax, st, 1LL << 24,
+                                     pctas, s);
+  else if (rc == LU_OK)
     rc = launch_gemm_bf16_tc(mL, mU, mC, 0, 0, 0, 0, M, N, Ke, bf16, bf16 ? nullptr : amax, st, 1LL << 24, s);
   DevStatus hst{};
   cudaMemcpyAsync(&hst, st, sizeof(hst), cudaMemcpyDeviceToHost, s);

@@ -48,7 +48,13 @@ struct lu_handle_s {
   cudaEvent_t evFork = nullptr, evP = nullptr, evN = nullptr;
   // leaf tuning: recursion leaf width and CTA cap, without / with look-ahead
   int leaf_w64 = 32, leaf_w32 = 64, leaf_ctas = 148;
-  int leaf_w64_la = 16, leaf_w32_la = 32, leaf_ctas_la = 64;
+  int leaf_w64_la = 16, leaf_w32_la = 32, leaf_ctas_la = 48;
+  // low-precision trailing update: CTAs of the persistent kernel (0: one CTA
+  // per tile); under look-ahead the update beside a running panel leaves
+  // gemm_reserve SMs to it
+  // (B200, N = 65536, FP16x3 with look-ahead: 48 SMs reserved and a 48-CTA
+  // leaf measured best)
+  int gemm_ctas = 148, gemm_reserve = 48;
   int32_t* perm = nullptr;
   int32_t* perm_work = nullptr;
   int* trsv_flags = nullptr;

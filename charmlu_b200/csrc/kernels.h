@@ -35,11 +35,14 @@ constexpr int kMaxLeafW = 64;
 template <typename T>
 int leaf_init();
 // Factor P[0:M, 0:ncols] (row-major, P = diagonal of the first column) with
-// partial pivoting; ipiv[j] = row_base + local pivot row.
+// partial pivoting; ipiv[j] = row_base + local pivot row.  Each swap is also
+// applied to the enclosing panel's other columns: prow0 points at the
+// panel's first column in the leaf's top row, the panel is pw wide and the
+// leaf starts lc0 columns in (prow0 = null: the leaf is the panel).
 template <typename T>
 int launch_getf2_leaf(T* P, int64_t lda, int M, int ncols, int32_t* ipiv, int row_base, const LeafScratch<T>& scr,
                       unsigned* bar, DevStatus* st, int info_base, double thr, long long spin, int max_ctas,
-                      cudaStream_t s);
+                      cudaStream_t s, T* prow0 = nullptr, int pw = 0, int lc0 = 0);
 
 // ---- pivot batches: compose sequential swaps into (dst <- src) lists
 // batch: swaps (k0+i) <-> ipiv[k0+i] for i in [0, cnt), cnt <= kMaxBatch
@@ -105,6 +108,10 @@ int gemm_bf16_init();
 int launch_gemm_bf16_tc(const CUtensorMap& mapA, const CUtensorMap& mapB, const CUtensorMap& mapC, int a_row0,
                         int b_row0, int c_row0, int c_col0, int M, int N, int K, bool bf16, const unsigned* amax,
                         DevStatus* st, long long spin, cudaStream_t s);
+// persistent variant: max_ctas CTAs walk the tiles (TMEM double-buffered)
+int launch_gemm_lowp_persistent(const CUtensorMap& mapA, const CUtensorMap& mapB, const CUtensorMap& mapC,
+                                int a_row0, int b_row0, int c_row0, int c_col0, int M, int N, int K, bool bf16,
+                                const unsigned* amax, DevStatus* st, long long spin, int max_ctas, cudaStream_t s);
 // |max| of the L21 (rows x K) and U12 (K x N) FP32 panels into amax[0], amax[1]
 int launch_panel_absmax(const float* L, int64_t ldl, int rows, int K, const float* U, int64_t ldu, int N,
                         unsigned* amax, cudaStream_t s);

@@ -135,23 +135,23 @@ int trsm64(Ctx64& c, const MatF64& Lm, int r0, int w, const MatF64& Bm, int rb, 
   return trsm64(c, Lm, r0 + w1, w - w1, Bm, rb + w1, cb, ncols);
 }
 
-// recursive panel factorisation of columns [c0, c0+w), rows [c0, n)
-int panel64(Ctx64& c, int c0, int w) {
+// recursive panel factorisation of columns [c0, c0+w), rows [c0, n), inside
+// the panel [p0, p0+pw): the leaves apply their row swaps to all of the
+// panel's columns, so the recursion needs no separate laswp
+int panel64(Ctx64& c, int c0, int w, int p0, int pw) {
   const int M = c.n - c0;
   if (w <= c.leaf_w) {
     unsigned* bar = c.h->take_counter();
     if (!bar) return LU_ERR_NOMEM;
     Prof pf(c.h, c.s, LU_PH_PANEL, (double)M * w * w);
     return launch_getf2_leaf<double>(c.A.at(c0, c0), c.A.ld, M, w, c.ipiv + c0, c0, c.h->leaf64, bar, c.h->st, c0,
-                                     c.thr, c.h->spin, c.leaf_ctas, c.s);
+                                     c.thr, c.h->spin, c.leaf_ctas, c.s, c.A.at(c0, p0), pw, c0 - p0);
   }
   const int w1 = split_w(w), w2 = w - w1;
-  LUB_TRY(panel64(c, c0, w1));
-  LUB_TRY(pivots_apply_f64(c, c0, w1, c0 + w1, c0 + w, 0, 0, nullptr, nullptr));
+  LUB_TRY(panel64(c, c0, w1, p0, pw));
   LUB_TRY(trsm64(c, c.A, c0, w1, c.A, c0, c0 + w1, w2));
   LUB_TRY(gemm64(c, c.A, c0 + w1, c0 + w1, c.A, c0 + w1, c0, c.A, c0, c0 + w1, M - w1, w2, w1));
-  LUB_TRY(panel64(c, c0 + w1, w2));
-  return pivots_apply_f64(c, c0 + w1, w2, c0, c0 + w1, 0, 0, nullptr, nullptr);
+  return panel64(c, c0 + w1, w2, p0, pw);
 }
 
 int check_common(lu_handle h, const void* dA, int64_t lda) {
@@ -185,7 +185,7 @@ int factor_f64_schedule(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, dou
   if (!la) {
     for (int k0 = 0; k0 < n; k0 += b) {
       const int kw = std::min(b, n - k0);
-      LUB_TRY(panel64(c, k0, kw));
+      LUB_TRY(panel64(c, k0, kw, k0, kw));
       LUB_TRY(pivots_apply_f64(c, k0, kw, 0, n, k0, k0 + kw, rhs, h->perm));
       const int rest = n - k0 - kw;
       if (rest > 0) {
@@ -204,7 +204,7 @@ int factor_f64_schedule(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, dou
   cp.pl = h->plistP;
   LUB_CUDA(cudaEventRecord(h->evFork, s));
   LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evFork, 0));
-  LUB_TRY(panel64(cp, 0, std::min(b, n)));
+  LUB_TRY(panel64(cp, 0, std::min(b, n), 0, std::min(b, n)));
   LUB_CUDA(cudaEventRecord(h->evP, h->sP));
   for (int k0 = 0; k0 < n; k0 += b) {
     const int kw = std::min(b, n - k0), k1 = k0 + kw, rest = n - k1;
@@ -216,7 +216,7 @@ int factor_f64_schedule(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, dou
     LUB_TRY(gemm64(c, c.A, k1, k1, c.A, k1, k0, c.A, k0, k1, rest, nw, kw, LU_PH_GEMM));  // next panel's columns
     LUB_CUDA(cudaEventRecord(h->evN, s));
     LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evN, 0));
-    LUB_TRY(panel64(cp, k1, nw));
+    LUB_TRY(panel64(cp, k1, nw, k1, nw));
     LUB_CUDA(cudaEventRecord(h->evP, h->sP));
     if (rest > nw)
       LUB_TRY(gemm64(c, c.A, k1, k1 + nw, c.A, k1, k0, c.A, k0, k1 + nw, rest, rest - nw, kw, LU_PH_GEMM));
@@ -314,12 +314,15 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
       s = LU_ERR_CUDA;
   }
   h->leaf_ctas = h->num_sms;
+  h->gemm_ctas = h->num_sms;
   if (const char* e = getenv("LU_B200_LEAF_CTAS")) h->leaf_ctas = std::max(1, atoi(e));
   if (const char* e = getenv("LU_B200_LEAF_CTAS_LA")) h->leaf_ctas_la = std::max(1, atoi(e));
   if (const char* e = getenv("LU_B200_LEAF_W64")) h->leaf_w64 = std::min(32, std::max(2, atoi(e)));
   if (const char* e = getenv("LU_B200_LEAF_W64_LA")) h->leaf_w64_la = std::min(32, std::max(2, atoi(e)));
   if (const char* e = getenv("LU_B200_LEAF_W32")) h->leaf_w32 = std::min(64, std::max(4, atoi(e)));
   if (const char* e = getenv("LU_B200_LEAF_W32_LA")) h->leaf_w32_la = std::min(64, std::max(4, atoi(e)));
+  if (const char* e = getenv("LU_B200_GEMM_CTAS")) h->gemm_ctas = std::max(0, atoi(e));
+  if (const char* e = getenv("LU_B200_GEMM_RESERVE")) h->gemm_reserve = std::max(0, atoi(e));
   if (s == LU_OK) s = h->alloc(&h->perm, n);
   if (s == LU_OK) s = h->alloc(&h->perm_work, n);
   if (s == LU_OK) s = h->alloc(&h->trsv_flags, n / 64 + 2);

@@ -95,22 +95,23 @@ int trsm32(Ctx32& c, int r0, int w, int rb, int cb, int ncols) {
   return trsm32(c, r0 + w1, w - w1, rb + w1, cb, ncols);
 }
 
-int panel32(Ctx32& c, int c0, int w) {
+// recursive FP32 panel of columns [c0, c0+w) inside the panel [p0, p0+pw);
+// the leaves swap rows across the whole panel (no laswp in the recursion)
+int panel32(Ctx32& c, int c0, int w, int p0, int pw) {
   const int M = c.n - c0;
   if (w <= c.leaf_w) {
     unsigned* bar = c.h->take_counter();
     if (!bar) return LU_ERR_NOMEM;
     Prof pf(c.h, c.s, LU_PH_PANEL, (double)M * w * w);
     return launch_getf2_leaf<float>(c.A + (int64_t)c0 * c.ld + c0, c.ld, M, w, c.ipiv + c0, c0, c.h->leaf32, bar,
-                                    c.h->st, c0, c.thr, c.h->spin, c.leaf_ctas, c.s);
+                                    c.h->st, c0, c.thr, c.h->spin, c.leaf_ctas, c.s, c.A + (int64_t)c0 * c.ld + p0,
+                                    pw, c0 - p0);
   }
   const int w1 = split_w32(w), w2 = w - w1;
-  LUB_TRY(panel32(c, c0, w1));
-  LUB_TRY(pivots_apply_f32(c, c0, w1, c0 + w1, c0 + w, 0, 0, nullptr));
+  LUB_TRY(panel32(c, c0, w1, p0, pw));
   LUB_TRY(trsm32(c, c0, w1, c0, c0 + w1, w2));
   LUB_TRY(sgemm(c, c0 + w1, c0 + w1, c0 + w1, c0, c0, c0 + w1, M - w1, w2, w1));
-  LUB_TRY(panel32(c, c0 + w1, w2));
-  return pivots_apply_f32(c, c0 + w1, w2, c0, c0 + w1, 0, 0, nullptr);
+  return panel32(c, c0 + w1, w2, p0, pw);
 }
 
 // Low-precision operand panels of step k (L21 rows k1.., U12^T) and their
@@ -141,11 +142,15 @@ int build_operands(lu_handle h, const Ctx32& c, int k0, int kw, int k1, int rest
 }
 
 // C(k1.., c0..c0+ncols) -= L21 * U12[:, u0..u0+ncols] on the tensor cores
+// (reserve: SMs left free for a panel running beside it)
 int lowp_gemm(lu_handle h, const CUtensorMap& mapL, const CUtensorMap& mapU, const CUtensorMap& mapC, int k1,
-              int rest, int u0, int ncols, int ke, bool bf16, cudaStream_t s) {
+              int rest, int u0, int ncols, int ke, bool bf16, cudaStream_t s, int reserve = 0) {
   Prof pf(h, s, LU_PH_GEMM, 2.0 * rest * (double)ncols * ke);
-  return launch_gemm_bf16_tc(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, ke, bf16, bf16 ? nullptr : h->amax,
-                             h->st, h->spin, s);
+  const unsigned* amax = bf16 ? nullptr : h->amax;
+  if (h->gemm_ctas > 0)
+    return launch_gemm_lowp_persistent(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, ke, bf16, amax, h->st,
+                                       h->spin, std::max(1, h->gemm_ctas - reserve), s);
+  return launch_gemm_bf16_tc(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, ke, bf16, amax, h->st, h->spin, s);
 }
 
 // LU of h->A32 in place: FP32 panels/TRSM, low-precision tcgen05 trailing
@@ -165,7 +170,7 @@ int factor_mixed(lu_handle h, cudaStream_t s) {
   if (!la) {
     for (int k0 = 0; k0 < n; k0 += B) {
       const int kw = std::min(B, n - k0);
-      LUB_TRY(panel32(c, k0, kw));
+      LUB_TRY(panel32(c, k0, kw, k0, kw));
       LUB_TRY(pivots_apply_f32(c, k0, kw, 0, n, k0, k0 + kw, h->perm));
       const int k1 = k0 + kw, rest = n - k1;
       if (rest <= 0) continue;
@@ -181,7 +186,7 @@ int factor_mixed(lu_handle h, cudaStream_t s) {
   cp.pl = h->plistP;
   LUB_CUDA(cudaEventRecord(h->evFork, s));
   LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evFork, 0));
-  LUB_TRY(panel32(cp, 0, std::min(B, n)));
+  LUB_TRY(panel32(cp, 0, std::min(B, n), 0, std::min(B, n)));
   LUB_CUDA(cudaEventRecord(h->evP, h->sP));
   for (int k0 = 0; k0 < n; k0 += B) {
     const int kw = std::min(B, n - k0), k1 = k0 + kw, rest = n - k1;
@@ -195,9 +200,9 @@ int factor_mixed(lu_handle h, cudaStream_t s) {
     LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, 0, nw, ke, bf16, s));  // next panel's columns
     LUB_CUDA(cudaEventRecord(h->evN, s));
     LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evN, 0));
-    LUB_TRY(panel32(cp, k1, nw));
+    LUB_TRY(panel32(cp, k1, nw, k1, nw));
     LUB_CUDA(cudaEventRecord(h->evP, h->sP));
-    if (rest > nw) LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, nw, rest - nw, ke, bf16, s));
+    if (rest > nw) LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, nw, rest - nw, ke, bf16, s, h->gemm_reserve));
   }
   return LU_OK;
 }

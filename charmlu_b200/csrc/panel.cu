@@ -11,6 +11,8 @@
 //                                       next-column update + candidate)
 //   updateLsubBlock (dger, offset 2)    lu.C:230-254
 //   singularity check                   lu.ci:339-341 (reported, not aborted)
+//   the row swap on the rest of the panel's columns (the reference swaps
+//   whole rows of the panel block, lu.ci:302-323)
 //
 // Design: a cooperative grid of G CTAs, each holding a contiguous range of
 // the panel's rows in shared memory for the whole launch (row pitch W+1 so a
@@ -68,7 +70,8 @@ __device__ __forceinline__ void block_argmax(T v, int r, T* s_v, int* s_r, T& ou
 template <typename T, int W>
 __global__ void __launch_bounds__(THREADS, 1)
 getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int row_base, LeafScratch<T> scr,
-                  unsigned* bar, DevStatus* st, int info_base, double thr, long long spin) {
+                  unsigned* bar, DevStatus* st, int info_base, double thr, long long spin, T* prow0, int pw,
+                  int lc0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int LD = W + 1;
   T* a = reinterpret_cast<T*>(smem_raw);  // [R][LD]
@@ -139,6 +142,22 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
       if (p >= r_lo && p < r_hi) a[(p - r_lo) * LD + tid] = __ldcg(&scr.rowj[slot * kMaxLeafW + tid]);
       if (j >= r_lo && j < r_hi) a[(j - r_lo) * LD + tid] = urow[tid];
     }
+    // the swap on the enclosing panel's other columns (prow0: panel's first
+    // column in this leaf's top row, pw columns, the leaf at lc0): each CTA a
+    // slice; the next grid barrier orders consecutive swaps
+    if (p != j && pw > ncols) {
+      const int others = pw - ncols;
+      const int per = (others + G - 1) / G;
+      const int q0 = cta * per, q1 = min(others, q0 + per);
+      T* r1 = prow0 + (int64_t)j * lda;
+      T* r2 = prow0 + (int64_t)p * lda;
+      for (int q = q0 + tid; q < q1; q += THREADS) {
+        const int col = q < lc0 ? q : q + ncols;
+        const T t = r1[col];
+        r1[col] = r2[col];
+        r2[col] = t;
+      }
+    }
     const T piv = urow[j];
     if (cta == 0 && tid == 0) {
       ipiv[j] = row_base + p;
@@ -180,7 +199,7 @@ size_t leaf_smem(int R) { return (size_t)R * (W + 1) * sizeof(T) + W * sizeof(T)
 template <typename T, int W>
 int launch_leaf_w(T* P, int64_t lda, int M, int ncols, int32_t* ipiv, int row_base, const LeafScratch<T>& scr,
                   unsigned* bar, DevStatus* st, int info_base, double thr, long long spin, int max_ctas,
-                  cudaStream_t s) {
+                  cudaStream_t s, T* prow0, int pw, int lc0) {
   // rows per CTA: enough CTAs to spread the panel, capped by max_ctas and by
   // shared memory (R * (W+1) * sizeof(T) <= ~216 KB)
   const int max_rows = (int)((216 * 1024 - W * sizeof(T)) / ((W + 1) * sizeof(T)));
@@ -194,7 +213,7 @@ int launch_leaf_w(T* P, int64_t lda, int M, int ncols, int32_t* ipiv, int row_ba
   G = ceil_div(M, R);
   size_t smem = leaf_smem<T, W>(R);
   void* args[] = {&P, &lda, &M, &ncols, &R, &ipiv, &row_base, const_cast<LeafScratch<T>*>(&scr), &bar, &st,
-                  &info_base, &thr, &spin};
+                  &info_base, &thr, &spin, &prow0, &pw, &lc0};
   LUB_CUDA(cudaLaunchCooperativeKernel((const void*)getf2_leaf_kernel<T, W>, dim3(G), dim3(THREADS), args, smem, s));
   __atomic_add_fetch(&g_kernel_launches, 1, __ATOMIC_RELAXED);
   return LU_OK;
@@ -215,22 +234,33 @@ int leaf_init() {
 template <typename T>
 int launch_getf2_leaf(T* P, int64_t lda, int M, int ncols, int32_t* ipiv, int row_base, const LeafScratch<T>& scr,
                       unsigned* bar, DevStatus* st, int info_base, double thr, long long spin, int max_ctas,
-                      cudaStream_t s) {
+                      cudaStream_t s, T* prow0, int pw, int lc0) {
   if (M <= 0 || ncols <= 0) return LU_OK;
+  if (!prow0) {  // no enclosing panel: the leaf is the whole panel
+    prow0 = P;
+    pw = ncols;
+    lc0 = 0;
+  }
+  if (lc0 < 0 || lc0 + ncols > pw) return LU_ERR_ARG;
   if (ncols <= 16)
-    return launch_leaf_w<T, 16>(P, lda, M, ncols, ipiv, row_base, scr, bar, st, info_base, thr, spin, max_ctas, s);
+    return launch_leaf_w<T, 16>(P, lda, M, ncols, ipiv, row_base, scr, bar, st, info_base, thr, spin, max_ctas, s,
+                                prow0, pw, lc0);
   if (ncols <= 32)
-    return launch_leaf_w<T, 32>(P, lda, M, ncols, ipiv, row_base, scr, bar, st, info_base, thr, spin, max_ctas, s);
+    return launch_leaf_w<T, 32>(P, lda, M, ncols, ipiv, row_base, scr, bar, st, info_base, thr, spin, max_ctas, s,
+                                prow0, pw, lc0);
   if (ncols <= 64)
-    return launch_leaf_w<T, 64>(P, lda, M, ncols, ipiv, row_base, scr, bar, st, info_base, thr, spin, max_ctas, s);
+    return launch_leaf_w<T, 64>(P, lda, M, ncols, ipiv, row_base, scr, bar, st, info_base, thr, spin, max_ctas, s,
+                                prow0, pw, lc0);
   return LU_ERR_ARG;
 }
 
 template int leaf_init<double>();
 template int leaf_init<float>();
 template int launch_getf2_leaf<double>(double*, int64_t, int, int, int32_t*, int, const LeafScratch<double>&,
-                                       unsigned*, DevStatus*, int, double, long long, int, cudaStream_t);
+                                       unsigned*, DevStatus*, int, double, long long, int, cudaStream_t, double*,
+                                       int, int);
 template int launch_getf2_leaf<float>(float*, int64_t, int, int, int32_t*, int, const LeafScratch<float>&,
-                                      unsigned*, DevStatus*, int, double, long long, int, cudaStream_t);
+                                      unsigned*, DevStatus*, int, double, long long, int, cudaStream_t, float*, int,
+                                      int);
 
 }  // namespace lub

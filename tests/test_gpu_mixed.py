@@ -77,6 +77,27 @@ def test_gemm_lowp_tcgen05_matches_reference(cuda_dev, M, N, K, mode):
         assert (split - A.double() @ B.double()).abs().max().item() <= 1e-5 * 18.5 * K / 64
 
 
+@pytest.mark.parametrize("mode", [0, 2])
+@pytest.mark.parametrize("pctas", [1, 3, 116, 148])
+@pytest.mark.parametrize("M,N,K", [(300, 520, 256), (1100, 2100, 192), (4096, 4096, 256)])
+def test_gemm_lowp_persistent_matches_tile_kernel(cuda_dev, M, N, K, mode, pctas):
+    """The persistent kernel (CTAs walking tiles, two TMEM accumulators)
+    issues the same MMAs per tile as the one-tile-per-CTA kernel: the
+    results agree bit for bit."""
+    f = _lib()
+    g = torch.Generator(device="cuda").manual_seed(M + 3 * N + pctas)
+    A = torch.rand(M, K, device="cuda", generator=g, dtype=torch.float32) - 0.5
+    B = (torch.rand(K, N, device="cuda", generator=g, dtype=torch.float32) - 0.5) * 5.0
+    ldc = (N + 3) // 4 * 4
+    C0 = torch.rand(M, ldc, device="cuda", generator=g, dtype=torch.float32) - 0.5
+    C1 = C0.clone()
+    st = torch.cuda.current_stream().cuda_stream
+    assert f(A.data_ptr(), K, B.data_ptr(), N, C0.data_ptr(), ldc, M, N, K, mode, st) == 0
+    assert f(A.data_ptr(), K, B.data_ptr(), N, C1.data_ptr(), ldc, M, N, K, mode | (pctas << 8), st) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(C0, C1)
+
+
 def _refine(n, b, A_np=None, seed=42, mode=None, target=16.0, prec=None, lookahead=False):
     import charmlu_b200 as lu
     prec = lu.LU_PREC_FP16X3 if prec is None else prec
