@@ -300,6 +300,119 @@ def run_ksweep(args, rank, world):
     return 0
 
 
+def _timed(fn):
+    import torch
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return out, e0.elapsed_time(e1)
+
+
+def run_adjoint(args, rank, world):
+    """Adjoint of X = A^{-1} B: FP64 at N=4096 with 16
+    right-hand sides against the FP64 LAPACK gradient, then the mixed
+    forward (low-precision factors + FP64 refinement) with the FP64-refined
+    adjoint at N=32768 in factor-storing and refactor-in-backward modes,
+    against the FP64 GPU path's gradient."""
+    import scipy.linalg as sl
+    import torch
+    import charmlu_b200 as lu
+    if rank != 0:
+        return 0
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    k = 16
+    rows = []
+
+    def rel(a, b):
+        return float((a - b).abs().max() / b.abs().max())
+
+    # ---- FP64, N = 4096
+    n = args.adjoint_n
+    A = lu.generate_uniform(n, n, seed=42, stream_id=0, device=dev)
+    B = lu.generate_uniform(n, k, seed=42, stream_id=2, device=dev)
+    W = 2.0 * lu.generate_uniform(n, k, seed=42, stream_id=3, device=dev)
+    s = lu.LUSolver(lu.LUConfig(n, 256))
+    LU = A.clone()
+    for _ in range(2):  # warm, then timed
+        LU.copy_(A)
+        (ipiv, t_fac) = _timed(lambda: s.factor(LU))
+        X = B.clone()
+        _, t_sol = _timed(lambda: s.solve(LU, ipiv, X))
+        (gA, gB), t_adj = _timed(lambda: s.adjoint(LU, ipiv, X, W))
+    assert s.status() == 0
+    An, Wn = A.cpu().numpy(), W.cpu().numpy()
+    f = sl.lu_factor(An)
+    Xr = sl.lu_solve(f, B.cpu().numpy())
+    lam = sl.lu_solve(f, Wn, trans=1)
+    gA_ref, gB_ref = torch.from_numpy(-lam @ Xr.T), torch.from_numpy(lam)
+    flops = 2 * (2 * n * n * k) + 2 * n * n * k
+    rows.append({"case": f"fp64 N={n} nrhs={k}", "factor_ms": t_fac, "solve_ms": t_sol, "adjoint_ms": t_adj,
+                 "adjoint_tflops": flops / t_adj / 1e9,
+                 "adjoint_gbs": (2 * 8 * n * n + 8 * n * n) / t_adj / 1e6,
+                 "rel_err_gradA": rel(gA.cpu(), gA_ref), "rel_err_gradB": rel(gB.cpu(), gB_ref)})
+    print(json.dumps(rows[-1]), flush=True)
+    del A, B, W, LU, X, gA, gB, s
+    torch.cuda.empty_cache()
+
+    # ---- mixed forward + FP64-refined adjoint, N = 32768
+    n = args.adjoint_mixed_n
+    A = lu.generate_uniform(n, n, seed=42, stream_id=0, device=dev)
+    B = lu.generate_uniform(n, k, seed=42, stream_id=2, device=dev)
+    W = 2.0 * lu.generate_uniform(n, k, seed=42, stream_id=3, device=dev)
+    # FP64 reference gradient from the FP64 GPU path
+    s64 = lu.LUSolver(lu.LUConfig(n, 256, lookahead=True))
+    LU = A.clone()
+    ipiv, t64_fac = _timed(lambda: s64.factor(LU))
+    X64 = B.clone()
+    _, t64_sol = _timed(lambda: s64.solve(LU, ipiv, X64))
+    (gA64, gB64), t64_adj = _timed(lambda: s64.adjoint(LU, ipiv, X64, W))
+    assert s64.status() == 0
+    gA64 = gA64.cpu()
+    del LU, s64
+    torch.cuda.empty_cache()
+    rows.append({"case": f"fp64 reference N={n} nrhs={k}", "factor_ms": t64_fac, "solve_ms": t64_sol,
+                 "adjoint_ms": t64_adj, "forward_ms": t64_fac + t64_sol})
+    print(json.dumps(rows[-1]), flush=True)
+    prec = {"bf16": lu.LU_PREC_BF16, "fp16s": lu.LU_PREC_FP16S, "fp16x3": lu.LU_PREC_FP16X3}[args.precision]
+    cfg = lu.LUConfig(n, args.block_mixed, precision=prec, lookahead=True, ir_target=args.adjoint_target)
+    for mode in ("storing", "refactor"):
+        for rep in range(2):  # warm, then timed
+            s = lu.LUSolver(cfg)
+            _, t_fac = _timed(lambda: s.refine_factor(A))
+            (X, fi), t_app = _timed(lambda: s.refine_apply(A, B))
+            if mode == "refactor":
+                s.close()
+                s = lu.LUSolver(cfg)
+                _, t_ref = _timed(lambda: s.refine_factor(A))
+            else:
+                t_ref = 0.0
+            (gA, gB, bi), t_adj = _timed(lambda: s.refine_adjoint(A, X, W))
+            st = s.status()
+            s.close()
+            if rep == 0:
+                del gA, gB, X
+                torch.cuda.empty_cache()
+        rows.append({"case": f"mixed {args.precision} N={n} nrhs={k} {mode}", "status": st,
+                     "ir_target": args.adjoint_target,
+                     "forward_ms": t_fac + t_app, "refine_factor_ms": t_fac, "refine_apply_ms": t_app,
+                     "forward_ir_iterations": fi["iterations"], "forward_r_hpl": fi["r_hpl"],
+                     "backward_ms": t_ref + t_adj, "backward_refactor_ms": t_ref, "adjoint_ms": t_adj,
+                     "adjoint_ir_iterations": bi["iterations"], "adjoint_r_hpl": bi["r_hpl"],
+                     "rel_err_X_vs_fp64": rel(X, X64), "rel_err_gradB_vs_fp64": rel(gB, gB64),
+                     "rel_err_gradA_vs_fp64": rel(gA.cpu(), gA64),
+                     "speedup_fwd_bwd_vs_fp64": (t64_fac + t64_sol + t64_adj) / (t_fac + t_app + t_ref + t_adj)})
+        print(json.dumps(rows[-1]), flush=True)
+        del gA, gB, X
+        torch.cuda.empty_cache()
+    print(json.dumps({"metric": "adjoint of X = A^-1 B (FP64 and mixed-precision forward)", "rows": rows}),
+          flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -317,7 +430,10 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=8192)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="lu", choices=["lu", "batched", "ksweep"])
+    ap.add_argument("--workload", default="lu", choices=["lu", "batched", "ksweep", "adjoint"])
+    ap.add_argument("--adjoint-n", type=int, default=4096)
+    ap.add_argument("--adjoint-mixed-n", type=int, default=32768)
+    ap.add_argument("--adjoint-target", type=float, default=0.25)
     ap.add_argument("--ksweep-n", type=int, default=8192)
     ap.add_argument("--ksweep-iters", type=int, default=30)
     ap.add_argument("--batch-count", type=int, default=4096)
@@ -332,6 +448,8 @@ def main():
         return run_batched(args, rank, world)
     if args.workload == "ksweep":
         return run_ksweep(args, rank, world)
+    if args.workload == "adjoint":
+        return run_adjoint(args, rank, world)
 
     import torch
     import charmlu_b200 as lu

@@ -231,6 +231,50 @@ class LUSolver:
         return x, {k: getattr(info, k) for k, _ in info._fields_}
 
 
+    def refine_factor(self, A, stream=None):
+        """Low-precision factorisation of A kept in the handle for
+        refine_apply / refine_adjoint (lu_refine_factor; A untouched)."""
+        lda = self._check_matrix(A)
+        _check(self._L.lu_refine_factor(self._h, _ptr(A), lda, _stream(stream)), "lu_refine_factor")
+
+    def refine_apply(self, A, B, X=None, trans=False, stream=None):
+        """op(A) X = B (op = A^T with trans) by FP64 iterative refinement on
+        the kept low-precision factors (lu_refine_apply).  Returns (X, info)."""
+        lda = self._check_matrix(A)
+        _require_cuda(B, torch.float64, "B")
+        B2 = B.contiguous() if B.dim() == 2 else B.contiguous().view(-1, 1)
+        k = B2.shape[1]
+        if X is None:
+            X = torch.empty(B.shape, dtype=torch.float64, device=A.device)
+        X2 = X if X.dim() == 2 else X.view(-1, 1)
+        info = _lib.LuRefineInfo()
+        _check(self._L.lu_refine_apply(self._h, _ptr(A), lda, int(bool(trans)), _ptr(B2), B2.stride(0) if k > 1 else 1,
+                                       _ptr(X2), X2.stride(0) if k > 1 else 1, k, ctypes.byref(info),
+                                       _stream(stream)), "lu_refine_apply")
+        return X, {f: getattr(info, f) for f, _ in info._fields_}
+
+    def refine_adjoint(self, A, X, W, want_gradA=True, stream=None):
+        """Adjoint of X = A^{-1} B on the kept low-precision factors:
+        lambda = A^{-T} W by FP64 refinement, grad_A = -lambda X^T
+        (lu_refine_adjoint).  Returns (gradA or None, gradB, info)."""
+        lda = self._check_matrix(A)
+        n = self.n
+        for t, nm in ((X, "X"), (W, "W")):
+            _require_cuda(t, torch.float64, nm)
+        X2 = X.contiguous() if X.dim() == 2 else X.contiguous().view(-1, 1)
+        W2 = W.contiguous() if W.dim() == 2 else W.contiguous().view(-1, 1)
+        k = W2.shape[1]
+        gradB = torch.empty(W.shape, dtype=torch.float64, device=A.device)
+        gB = gradB if gradB.dim() == 2 else gradB.view(-1, 1)
+        gradA = torch.empty(n, n, dtype=torch.float64, device=A.device) if want_gradA else None
+        info = _lib.LuRefineInfo()
+        _check(self._L.lu_refine_adjoint(self._h, _ptr(A), lda, _ptr(X2), X2.stride(0) if k > 1 else 1, _ptr(W2),
+                                         W2.stride(0) if k > 1 else 1, k, _ptr(gB), gB.stride(0) if k > 1 else 1,
+                                         _ptr(gradA) if want_gradA else None, n, ctypes.byref(info),
+                                         _stream(stream)), "lu_refine_adjoint")
+        return gradA, gradB, {f: getattr(info, f) for f, _ in info._fields_}
+
+
 def launch_count():
     """Kernels liblu_b200 has launched since it was loaded."""
     return int(_lib.load().lu_launch_count())

@@ -21,7 +21,8 @@ EXPORTS = [
     "lu_solve", "lu_factor_solve", "lu_residual", "lu_refine_solve", "lu_adjoint",
     "lu_batched_factor_solve", "lu_generate_uniform", "lu_matgen_host", "lu_status_string",
     "lu_profile", "lu_phase_times", "lu_launch_count", "lu_solve_noalloc",
-    "lu_batched_work_bytes", "lu_batched_set_tuning",
+    "lu_batched_work_bytes", "lu_batched_set_tuning", "lu_refine_factor", "lu_refine_apply",
+    "lu_refine_adjoint",
 ]
 PHASES = ["panel", "laswp", "trsm", "gemm", "gemm_inner", "solve", "other"]
 
@@ -70,6 +71,10 @@ def load():
         "lu_residual": ([H, P, i64, P, P, ctypes.POINTER(LuResidualInfo), P], ctypes.c_int),
         "lu_refine_solve": ([H, P, i64, P, P, ctypes.POINTER(LuRefineInfo), P], ctypes.c_int),
         "lu_adjoint": ([H, P, i64, P, P, i64, P, i64, i64, P, i64, P, i64, P], ctypes.c_int),
+        "lu_refine_factor": ([H, P, i64, P], ctypes.c_int),
+        "lu_refine_apply": ([H, P, i64, i32, P, i64, P, i64, i64, ctypes.POINTER(LuRefineInfo), P], ctypes.c_int),
+        "lu_refine_adjoint": ([H, P, i64, P, i64, P, i64, i64, P, i64, P, i64, ctypes.POINTER(LuRefineInfo), P],
+                              ctypes.c_int),
         "lu_batched_factor_solve": ([i32, P, P, P, P, P, P, i32, P, ctypes.c_size_t, P], ctypes.c_int),
         "lu_generate_uniform": ([P, i64, i64, i64, u64, u64, P], ctypes.c_int),
         "lu_matgen_host": ([P, i64, i32, i64], ctypes.c_int),

@@ -82,6 +82,19 @@ struct lu_handle_s {
   double* hdot = nullptr;      // GMRES dot-product partials / results
   int gm = 0;                  // GMRES restart length
   bool mixed_ready = false;
+  // factors kept for lu_refine_apply / lu_refine_adjoint
+  bool mixed_factored = false;
+  int32_t* perm32 = nullptr;   // row permutation of those factors
+  // multi-RHS refinement work blocks (ld 16), allocated on first use
+  double* mr_P = nullptr;      // residual partials, kMultiMaxSplits * n * 16
+  double* mr_Pn = nullptr;     // row-norm partials, kMultiMaxSplits * n
+  double* mr_R = nullptr;      // residual block
+  double* mr_D = nullptr;      // correction block
+  double* mr_X = nullptr;      // iterate
+  double* mr_S = nullptr;      // GMRES: operand staging block (column 0 only)
+  double* mr_T = nullptr;      // GMRES: product block
+  double* mr_dc = nullptr;     // GMRES: correction of one column
+  unsigned long long* mr_acc = nullptr;
   std::vector<void*> allocs;
   size_t bytes = 0;
   long long spin = 0;

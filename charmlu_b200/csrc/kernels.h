@@ -73,9 +73,28 @@ int launch_trsv(const T* LU, int64_t lda, int n, T* x, int upper, int* flags, un
                 long long spin, cudaStream_t s);
 
 // multi-RHS pipelined triangular solve (mode 0 L, 1 U, 2 U^T, 3 L^T) on a
-// row-major n x nrhs block
-int launch_trsm_pipe(const double* LU, int64_t lda, int n, double* Y, int64_t ldy, int nrhs, int mode, int* flags,
+// row-major n x nrhs FP64 block; factors stored as TS (double or float)
+template <typename TS>
+int launch_trsm_pipe(const TS* LU, int64_t lda, int n, double* Y, int64_t ldy, int nrhs, int mode, int* flags,
                      unsigned* ticket, DevStatus* st, long long spin, cudaStream_t s);
+
+// ---- multi-RHS refinement (up to 16 columns, ld 16 work blocks)
+constexpr int kMultiMaxSplits = 16;  // reduction splits of the residual product
+constexpr int kMultiAccWords = 64;   // |R|, |B|, |X| maxima per column, ||op(A)||inf
+// number of splits S and their length for order n
+int multi_residual_splits(int n, int num_sms, int* split_len);
+// R = B - op(A) X (op = A^T when trans), per-column maxima into acc;
+// P: S * n * 16 doubles, Pn: S * n doubles of partials
+int launch_multi_residual(const double* A, int64_t lda, int n, int trans, const double* X, const double* B,
+                          int64_t ldb, int nrhs, double* R, double* P, double* Pn, int S, int split_len, int norm,
+                          unsigned long long* acc, cudaStream_t s);
+// X[dst(i)] += D[i] (dst = perm[i] with scatter, else i), ld 16
+int launch_multi_add(double* X, const double* D, const int32_t* perm, int n, int nrhs, int scatter, cudaStream_t s);
+// single columns of ld-16 blocks: out[i] = M[perm ? perm[i] : i][c] * scale;
+// dst[perm[i]] = src[i]; M[i][c] = v[i] (assign) or += v[i]
+int launch_col_get(const double* M, int c, const int32_t* perm, double* out, int n, double scale, cudaStream_t s);
+int launch_vec_scatter(const double* src, const int32_t* perm, double* dst, int n, cudaStream_t s);
+int launch_col_put(double* M, int c, const double* v, int n, int assign, cudaStream_t s);
 // G = -Lam X^T (rank k <= 16)
 int launch_neg_outer(const double* Lam, int64_t ldl, const double* X, int64_t ldx, int n, int k, double* G,
                      int64_t ldg, cudaStream_t s);

@@ -256,23 +256,22 @@ int device_status(lu_handle h, cudaStream_t s) {
   return st.code != 0 ? st.code : st.info;
 }
 
-// Left-preconditioned GMRES on the correction: M^{-1} A d = M^{-1} r with
-// M = P^T L U (FP32 factors applied in FP64), FP64 Arnoldi with two passes of
-// classical Gram-Schmidt.  x += d.
-// rnorm: ||r||inf of the residual in h->r64 (the start vector is built from
-// r / rnorm, so the Krylov right-hand side is beta * rnorm).
-int gmres_correction(lu_handle h, const double* A, int64_t lda, double* x, double rnorm, cudaStream_t s,
-                     int* iters_out) {
+// Left-preconditioned GMRES on the correction: M^{-1} op(A) d = M^{-1} r
+// with M the FP32 factors applied in FP64 arithmetic (which GMRES-IR's
+// convergence needs), FP64 Arnoldi with two passes of classical
+// Gram-Schmidt.  x += d.
+//   init(v0):       v0 = M^{-1} (r / rnorm)
+//   op_prec(v, w):  w = M^{-1} op(A) v
+// rnorm: ||r||inf of the residual (the Krylov right-hand side is
+// beta * rnorm with beta = ||v0||2).
+template <class Init, class OpPrec>
+int gmres_cycle(lu_handle h, double* x, double rnorm, cudaStream_t s, int* iters_out, Init init, OpPrec op_prec) {
   const int n = (int)h->cfg.n, m = h->gm;
   double* V = h->V;
   double* part = h->hdot;
   double* hd = h->hdot + 128 * (m + 2);  // m + 2 doubles of results
   std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1, 0.0), hcol(m + 1);
-  // v0 = M^{-1} r / ||M^{-1} r||  (r already in h->r64, racc holds ||r||);
-  // the preconditioner is applied in working precision (FP64 vectors and
-  // arithmetic on the FP32 factors), which GMRES-IR's convergence needs
-  LUB_TRY(launch_gather_f64(h->r64, h->perm, V, n, 1.0, h->racc, s));
-  LUB_TRY(solve_f32_factors_f64(h, V, s));
+  LUB_TRY(init(V));
   LUB_TRY(launch_multi_dot(V, 1, V, n, part, hd, s));
   double beta2 = 0.0;
   LUB_CUDA(cudaMemcpyAsync(&beta2, hd, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -285,13 +284,7 @@ int gmres_correction(lu_handle h, const double* A, int64_t lda, double* x, doubl
   for (int j = 0; j < m; j++) {
     double* vj = V + (size_t)j * n;
     double* w = V + (size_t)(j + 1) * n;
-    // w = M^{-1} A v_j   (residual kernel with b = 0 gives -A v_j)
-    {
-      Prof pf(h, s, LU_PH_OTHER);
-      LUB_TRY(launch_residual_f64(A, lda, n, vj, h->zero64, h->z64, h->racc, s));
-    }
-    LUB_TRY(launch_gather_f64(h->z64, h->perm, w, n, -1.0, nullptr, s));
-    LUB_TRY(solve_f32_factors_f64(h, w, s));
+    LUB_TRY(op_prec(vj, w));
     // two passes of classical Gram-Schmidt
     std::fill(hcol.begin(), hcol.end(), 0.0);
     for (int pass = 0; pass < 2; pass++) {
@@ -339,18 +332,46 @@ int gmres_correction(lu_handle h, const double* A, int64_t lda, double* x, doubl
   return LU_OK;
 }
 
-int refine_solve(lu_handle h, const double* A, int64_t lda, const double* b, double* x, lu_refine_info* info,
-                 cudaStream_t s) {
+// GMRES cycle of the single-RHS solve A x = b (residual in h->r64, its
+// norms in h->racc)
+int gmres_correction(lu_handle h, const double* A, int64_t lda, double* x, double rnorm, cudaStream_t s,
+                     int* iters_out) {
+  const int n = (int)h->cfg.n;
+  auto init = [&](double* v0) {
+    LUB_TRY(launch_gather_f64(h->r64, h->perm, v0, n, 1.0, h->racc, s));
+    return solve_f32_factors_f64(h, v0, s);
+  };
+  auto op_prec = [&](const double* vj, double* w) {
+    {  // residual kernel with b = 0 gives -A v_j
+      Prof pf(h, s, LU_PH_OTHER);
+      LUB_TRY(launch_residual_f64(A, lda, n, vj, h->zero64, h->z64, h->racc, s));
+    }
+    LUB_TRY(launch_gather_f64(h->z64, h->perm, w, n, -1.0, nullptr, s));
+    return solve_f32_factors_f64(h, w, s);
+  };
+  return gmres_cycle(h, x, rnorm, s, iters_out, init, op_prec);
+}
+
+// FP32 working copy of A and its low-precision factorisation (h->A32,
+// h->perm); the status word is cleared first
+int mixed_factor(lu_handle h, const double* A, int64_t lda, cudaStream_t s) {
   const int n = (int)h->cfg.n;
   LUB_TRY(ensure_mixed(h));
   LUB_CUDA(cudaMemsetAsync(h->st, 0, sizeof(DevStatus), s));
-  LUB_TRY(run_graph(h, 1, A, h->A32, nullptr, lda, s, [&](cudaStream_t ss) {
+  return run_graph(h, 1, A, h->A32, nullptr, lda, s, [&](cudaStream_t ss) {
     {
       Prof pf(h, ss, LU_PH_OTHER);
       LUB_TRY(launch_f64_to_f32(A, lda, h->A32, h->ld32, n, n, ss));
     }
     return factor_mixed(h, ss);
-  }));
+  });
+}
+
+int refine_solve(lu_handle h, const double* A, int64_t lda, const double* b, double* x, lu_refine_info* info,
+                 cudaStream_t s) {
+  const int n = (int)h->cfg.n;
+  h->mixed_factored = false;
+  LUB_TRY(mixed_factor(h, A, lda, s));
   // x0 = U^{-1} L^{-1} P b in FP32
   LUB_TRY(launch_gather_f64_to_f32(b, h->perm, h->v32, n, 1.0, s));
   LUB_TRY(solve32(h, h->v32, s));
@@ -401,7 +422,236 @@ int refine_solve(lu_handle h, const double* A, int64_t lda, const double* b, dou
   return LU_OK;
 }
 
+// ---- multi-RHS refinement on kept factors --------------------------------
+
+int ensure_multi(lu_handle h) {
+  if (h->mr_acc) return LU_OK;
+  const size_t n = (size_t)h->cfg.n;
+  LUB_TRY(h->alloc(&h->mr_P, (size_t)kMultiMaxSplits * n * 16));
+  LUB_TRY(h->alloc(&h->mr_Pn, (size_t)kMultiMaxSplits * n));
+  LUB_TRY(h->alloc(&h->mr_R, n * 16));
+  LUB_TRY(h->alloc(&h->mr_D, n * 16));
+  LUB_TRY(h->alloc(&h->mr_X, n * 16));
+  LUB_TRY(h->alloc(&h->mr_S, n * 16));
+  LUB_TRY(h->alloc(&h->mr_T, n * 16));
+  LUB_TRY(h->alloc(&h->mr_dc, n));
+  LUB_TRY(h->alloc(&h->mr_acc, kMultiAccWords));
+  LUB_CUDA(cudaMemset(h->mr_S, 0, sizeof(double) * n * 16));
+  return LU_OK;
+}
+
+// M^{-T} v in place for a contiguous vector (FP32 factors, FP64
+// arithmetic): v <- P^T L^{-T} U^{-T} v; tmp is n doubles of scratch
+int prec_trans_vec(lu_handle h, double* v, double* tmp, cudaStream_t s) {
+  const int n = (int)h->cfg.n;
+  Prof pf(h, s, LU_PH_SOLVE, 2.0 * n * (double)n);
+  LUB_CUDA(cudaMemcpyAsync(tmp, v, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  LUB_TRY(launch_trsm_pipe<float>(h->A32, h->ld32, n, tmp, 1, 1, 2, h->trsv_flags, h->trsv_ticket, h->st, h->spin,
+                                  s));
+  LUB_TRY(launch_trsm_pipe<float>(h->A32, h->ld32, n, tmp, 1, 1, 3, h->trsv_flags, h->trsv_ticket, h->st, h->spin,
+                                  s));
+  return launch_vec_scatter(tmp, h->perm32, v, n, s);
+}
+
+// One GMRES cycle on column c of a refinement group: residual in
+// h->mr_R[:, c] (||r||inf = rnorm), correction added to h->mr_X[:, c]
+int multi_gmres_column(lu_handle h, const double* A, int64_t lda, int trans, int c, double rnorm, int S,
+                       int split_len, cudaStream_t s, int* iters) {
+  const int n = (int)h->cfg.n;
+  auto init = [&](double* v0) {
+    if (!trans) {
+      LUB_TRY(launch_col_get(h->mr_R, c, h->perm32, v0, n, 1.0 / rnorm, s));
+      return solve_f32_factors_f64(h, v0, s);
+    }
+    LUB_TRY(launch_col_get(h->mr_R, c, nullptr, v0, n, 1.0 / rnorm, s));
+    return prec_trans_vec(h, v0, h->z64, s);
+  };
+  auto op_prec = [&](const double* vj, double* w) {
+    if (!trans) {
+      {  // residual kernel with b = 0 gives -A v_j
+        Prof pf(h, s, LU_PH_OTHER);
+        LUB_TRY(launch_residual_f64(A, lda, n, vj, h->zero64, h->z64, h->racc, s));
+      }
+      LUB_TRY(launch_gather_f64(h->z64, h->perm32, w, n, -1.0, nullptr, s));
+      return solve_f32_factors_f64(h, w, s);
+    }
+    LUB_TRY(launch_col_put(h->mr_S, 0, vj, n, 1, s));
+    {  // R = 0 - A^T v_j in column 0
+      Prof pf(h, s, LU_PH_OTHER);
+      LUB_TRY(launch_multi_residual(A, lda, n, 1, h->mr_S, h->zero64, 1, 1, h->mr_T, h->mr_P, h->mr_Pn, S,
+                                    split_len, 0, h->mr_acc, s));
+    }
+    LUB_TRY(launch_col_get(h->mr_T, 0, nullptr, w, n, -1.0, s));
+    return prec_trans_vec(h, w, h->z64, s);
+  };
+  LUB_CUDA(cudaMemsetAsync(h->mr_dc, 0, sizeof(double) * n, s));
+  LUB_TRY(gmres_cycle(h, h->mr_dc, rnorm, s, iters, init, op_prec));
+  return launch_col_put(h->mr_X, c, h->mr_dc, n, 0, s);
+}
+
+// x += op(A)^{-1} r through the FP32 factors (FP64 vectors and arithmetic):
+//   op = A:   P^T L U d = r   ->  d = U^{-1} L^{-1} (P r)
+//   op = A^T: U^T L^T P d = r ->  d = P^T L^{-T} U^{-T} r
+// r (h->mr_R) is overwritten in the transposed case.
+int multi_correction(lu_handle h, int trans, int k, cudaStream_t s) {
+  const int n = (int)h->cfg.n;
+  Prof pf(h, s, LU_PH_SOLVE, 2.0 * n * (double)n * k);
+  if (!trans) {
+    LUB_TRY(launch_permute_rows(h->mr_R, 16, h->mr_D, 16, h->perm32, n, k, 0, s));
+    LUB_TRY(launch_trsm_pipe<float>(h->A32, h->ld32, n, h->mr_D, 16, k, 0, h->trsv_flags, h->trsv_ticket, h->st,
+                                    h->spin, s));
+    LUB_TRY(launch_trsm_pipe<float>(h->A32, h->ld32, n, h->mr_D, 16, k, 1, h->trsv_flags, h->trsv_ticket, h->st,
+                                    h->spin, s));
+    return launch_multi_add(h->mr_X, h->mr_D, h->perm32, n, k, 0, s);
+  }
+  LUB_TRY(launch_trsm_pipe<float>(h->A32, h->ld32, n, h->mr_R, 16, k, 2, h->trsv_flags, h->trsv_ticket, h->st,
+                                  h->spin, s));
+  LUB_TRY(launch_trsm_pipe<float>(h->A32, h->ld32, n, h->mr_R, 16, k, 3, h->trsv_flags, h->trsv_ticket, h->st,
+                                  h->spin, s));
+  return launch_multi_add(h->mr_X, h->mr_R, h->perm32, n, k, 1, s);
+}
+
+// op(A) X = B for k <= 16 columns: low-precision solve, then classical IR
+// with the FP64 residual until every column's scaled residual is below the
+// target; when classical steps stop contracting (or cfg.ir_mode asks for
+// it) each column still above the target gets GMRES-IR cycles instead.
+// ri reports the worst column.
+int refine_group(lu_handle h, const double* A, int64_t lda, int trans, const double* B, int64_t ldb, double* X,
+                 int64_t ldx, int k, lu_refine_info* ri, cudaStream_t s) {
+  const int n = (int)h->cfg.n;
+  int split_len = 0;
+  const int S = multi_residual_splits(n, h->num_sms, &split_len);
+  LUB_CUDA(cudaMemsetAsync(h->mr_X, 0, sizeof(double) * n * 16, s));
+  LUB_CUDA(cudaMemcpy2DAsync(h->mr_R, 16 * sizeof(double), B, ldb * sizeof(double), k * sizeof(double), n,
+                             cudaMemcpyDeviceToDevice, s));
+  LUB_TRY(multi_correction(h, trans, k, s));
+  const double target = h->cfg.ir_target > 0 ? h->cfg.ir_target : 16.0;
+  const int max_it = h->cfg.ir_max_iter > 0 ? h->cfg.ir_max_iter : 50;
+  const double eps = 2.220446049250313e-16;
+  double anorm = 0.0, prev = INFINITY, worst = INFINITY;
+  unsigned long long acc[kMultiAccWords];
+  double rc[16], rn[16];
+  bool gm = h->cfg.ir_mode == LU_IR_GMRES;
+  int gm_stall = 0;
+  for (int it = 0;; it++) {
+    {
+      Prof pf(h, s, LU_PH_OTHER, 2.0 * n * (double)n * k);
+      LUB_TRY(launch_multi_residual(A, lda, n, trans, h->mr_X, B, ldb, k, h->mr_R, h->mr_P, h->mr_Pn, S, split_len,
+                                    it == 0, h->mr_acc, s));
+    }
+    LUB_CUDA(cudaMemcpyAsync(acc, h->mr_acc, sizeof(acc), cudaMemcpyDeviceToHost, s));
+    LUB_CUDA(cudaStreamSynchronize(s));
+    if (it == 0) anorm = bits_to_double(acc[48]);
+    worst = 0.0;
+    for (int c = 0; c < k; c++) {
+      rn[c] = bits_to_double(acc[c]);
+      rc[c] = rn[c] / ((anorm * bits_to_double(acc[32 + c]) + bits_to_double(acc[16 + c])) * (double)n * eps);
+      worst = (rc[c] > worst || std::isnan(rc[c])) ? rc[c] : worst;
+    }
+    if (it == 0) ri->r_hpl_initial = std::max(ri->r_hpl_initial, worst);
+    if (!std::isfinite(worst) || worst < target || it >= max_it) break;
+    if (!gm && it >= 2 && worst > 0.5 * prev) gm = true;  // classical IR stopped contracting
+    // GMRES cycles that no longer reduce the residual: the low-precision
+    // factors have lost too much of A's spectrum; report non-convergence
+    if (ri->used_gmres) gm_stall = (worst > 0.9 * prev) ? gm_stall + 1 : 0;
+    if (gm_stall >= 3) break;
+    prev = worst;
+    if (gm) {
+      for (int c = 0; c < k; c++) {
+        if (!(rc[c] >= target) || !(rn[c] > 0.0)) continue;
+        int iters = 0;
+        LUB_TRY(multi_gmres_column(h, A, lda, trans, c, rn[c], S, split_len, s, &iters));
+        ri->used_gmres = 1;
+        ri->gmres_iterations += iters;
+      }
+    } else {
+      LUB_TRY(multi_correction(h, trans, k, s));
+      ri->iterations++;
+    }
+  }
+  if (!(worst <= ri->r_hpl)) ri->r_hpl = worst;  // worst over groups (NaN sticks)
+  if (!(std::isfinite(worst) && worst < target)) ri->status = LU_ERR_NOCONV;
+  LUB_CUDA(cudaMemcpy2DAsync(X, ldx * sizeof(double), h->mr_X, 16 * sizeof(double), k * sizeof(double), n,
+                             cudaMemcpyDeviceToDevice, s));
+  return LU_OK;
+}
+
+int refine_apply(lu_handle h, const double* A, int64_t lda, int trans, const double* B, int64_t ldb, double* X,
+                 int64_t ldx, int64_t nrhs, lu_refine_info* info, cudaStream_t s) {
+  lu_refine_info ri;
+  memset(&ri, 0, sizeof(ri));
+  ri.r_hpl = 0.0;
+  const int fst = device_status(h, s);
+  if (fst != LU_OK) {  // singular factors or an earlier device error
+    ri.status = fst;
+    if (info) *info = ri;
+    return LU_OK;
+  }
+  LUB_TRY(ensure_multi(h));
+  for (int64_t c0 = 0; c0 < nrhs; c0 += 16) {
+    const int k = (int)std::min<int64_t>(16, nrhs - c0);
+    LUB_TRY(refine_group(h, A, lda, trans, B + c0, ldb, X + c0, ldx, k, &ri, s));
+  }
+  if (ri.status == LU_OK) {
+    const int st = device_status(h, s);
+    if (st != LU_OK) ri.status = st;
+  } else {
+    int code = ri.status;
+    LUB_CUDA(cudaMemcpyAsync(&h->st->code, &code, sizeof(int), cudaMemcpyHostToDevice, s));
+  }
+  if (info) *info = ri;
+  return LU_OK;
+}
+
+int check_refine_args(lu_handle h, const double* dA, int64_t lda) {
+  if (!h || !dA || lda < h->cfg.n) return LU_ERR_ARG;
+  if (h->cfg.precision == LU_PREC_FP64 || h->cfg.precision == LU_PREC_FP32) return LU_ERR_UNSUPPORTED;
+  if (h->cfg.block_size % 64) return LU_ERR_ARG;  // whole 64-wide k-blocks per panel
+  return LU_OK;
+}
+
 }  // namespace
+
+extern "C" int lu_refine_factor(lu_handle h, const double* dA, int64_t lda, void* stream) {
+  LUB_TRY(check_refine_args(h, dA, lda));
+  LUB_TRY(ensure_kernels_init());
+  cudaStream_t s = (cudaStream_t)stream;
+  h->mixed_factored = false;
+  LUB_TRY(mixed_factor(h, dA, lda, s));
+  if (!h->perm32) LUB_TRY(h->alloc(&h->perm32, h->cfg.n));
+  LUB_CUDA(cudaMemcpyAsync(h->perm32, h->perm, sizeof(int32_t) * h->cfg.n, cudaMemcpyDeviceToDevice, s));
+  h->mixed_factored = true;
+  return LU_OK;
+}
+
+extern "C" int lu_refine_apply(lu_handle h, const double* dA, int64_t lda, int trans, const double* dB, int64_t ldb,
+                               double* dX, int64_t ldx, int64_t nrhs, lu_refine_info* info, void* stream) {
+  LUB_TRY(check_refine_args(h, dA, lda));
+  if (!dB || !dX || nrhs < 1 || ldb < nrhs || ldx < nrhs || (trans != 0 && trans != 1)) return LU_ERR_ARG;
+  if ((lda & 1) || (reinterpret_cast<uintptr_t>(dA) & 15)) return LU_ERR_ALIGN;
+  if (!h->mixed_factored) return LU_ERR_ARG;  // no lu_refine_factor on this handle
+  return refine_apply(h, dA, lda, trans, dB, ldb, dX, ldx, nrhs, info, (cudaStream_t)stream);
+}
+
+extern "C" int lu_refine_adjoint(lu_handle h, const double* dA, int64_t lda, const double* dX, int64_t ldx,
+                                 const double* dW, int64_t ldw, int64_t nrhs, double* gradB, int64_t ldgb,
+                                 double* gradA, int64_t ldga, lu_refine_info* info, void* stream) {
+  LUB_TRY(check_refine_args(h, dA, lda));
+  if (!dX || !dW || !gradB || nrhs < 1 || ldx < nrhs || ldw < nrhs || ldgb < nrhs) return LU_ERR_ARG;
+  if (gradA && ldga < h->cfg.n) return LU_ERR_ARG;
+  if ((lda & 1) || (reinterpret_cast<uintptr_t>(dA) & 15)) return LU_ERR_ALIGN;
+  if (!h->mixed_factored) return LU_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  lu_refine_info ri;
+  LUB_TRY(refine_apply(h, dA, lda, 1, dW, ldw, gradB, ldgb, nrhs, &ri, s));
+  if (info) *info = ri;
+  if (gradA && ri.status == LU_OK) {
+    const int n = (int)h->cfg.n;
+    Prof pf(h, s, LU_PH_OTHER, 2.0 * n * (double)n * nrhs);
+    LUB_TRY(launch_neg_outer(gradB, ldgb, dX, ldx, n, (int)nrhs, gradA, ldga, s));
+  }
+  return LU_OK;
+}
 
 extern "C" int lu_refine_solve(lu_handle h, const double* dA, int64_t lda, const double* db, double* dx,
                                lu_refine_info* info, void* stream) {

@@ -8,12 +8,16 @@
 // substitution of one right-hand side, restating forwardSolve /
 // backwardSolve / offDiagSolve (lu.ci:387-458).  The reference pipelines
 // block rows through multicasts and a row-sum reduction into the diagonal
-// chare; here one CTA per 64-row block takes a ticket in launch order, reads
-// its row block of the factor while earlier blocks finish, waits (bounded)
-// on each earlier block's ready flag, accumulates the off-diagonal product,
-// then one warp substitutes inside the diagonal block and publishes the
-// block with a release flag.  A CTA only ever waits on lower tickets, which
-// were handed to CTAs already running, so the pipeline cannot deadlock.
+// chare; here one CTA per 64-row block takes a ticket in launch order and,
+// before it joins the chain, reads its right-hand side and diagonal tile
+// and inverts that tile.  It then accumulates the off-diagonal product as
+// earlier blocks become final (a progress counter: CTAs finish in ticket
+// order), applies the inverted tile (a 64 x 64 matrix-vector product, so
+// the sequential part of each chain step is short) and publishes its rows.
+// The reference's per-row division by u_ii happens inside the tile
+// inversion; the result differs from plain substitution by rounding only.
+// A CTA only ever waits on lower tickets, which were handed to CTAs already
+// running, so the pipeline cannot deadlock.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -46,14 +50,79 @@ __global__ void __launch_bounds__(128) trsm_llu_leaf_kernel(const T* L, int64_t 
 
 constexpr int TB = 64;  // rows per TRSV block
 
+// Inverse of the diagonal tile, computed by each pipeline CTA before it
+// joins the chain (it depends on nothing else), so that the chain step
+// itself is a 64 x 64 matrix-vector product instead of a 64-step
+// substitution.  D: the tile as stored (element (i, j) at D[i * ldd + j]),
+// unit lower (UPPER = false; the diagonal is not read) or upper; rows past
+// `rows` are treated as identity.  Four threads per column (256 threads),
+// rows in dependency order:
+//   lower: Dinv[i][j] = -sum_{j <= k < i} D[i][k] Dinv[k][j]
+//   upper: Dinv[i][j] = (delta_ij - sum_{i < k <= j} D[i][k] Dinv[k][j]) / D[i][i]
+template <bool UPPER, typename TD, typename TI>
+__device__ void tri_inverse_tile(const TD* D, int ldd, TI* Dinv, int ldi, int rows) {
+  const int tid = threadIdx.x, j = tid >> 2, q = tid & 3;
+  for (int step = 0; step < TB; step++) {
+    const int i = UPPER ? TB - 1 - step : step;
+    const bool live = i < rows && (UPPER ? i <= j : i > j);
+    TI s = TI(0);
+    if (live) {
+      if (UPPER) {
+        for (int k = i + 1 + q; k <= j; k += 4) s = fma((TI)D[i * ldd + k], Dinv[k * ldi + j], s);
+      } else {
+        for (int k = j + q; k < i; k += 4) s = fma((TI)D[i * ldd + k], Dinv[k * ldi + j], s);
+      }
+    }
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    TI v;
+    if (!live) v = (i == j) ? TI(1) : TI(0);
+    else if (UPPER) v = ((i == j ? TI(1) : TI(0)) - s) / (TI)D[i * ldd + i];
+    else v = -s;
+    if (q == 0) Dinv[i * ldi + j] = v;
+    __syncwarp();
+  }
+}
+
+// Pipeline progress: CTAs finish in ticket order (each waits for its
+// predecessor), so one counter, set to ticket + 1 when a CTA has published
+// its rows, tells every later CTA how many blocks are final.  A waiter far
+// behind the front sleeps in proportion to its distance, which keeps the
+// polls on that one word sparse.  Bounded: false after `spin` polls or when
+// another CTA has recorded an error.
+__device__ __forceinline__ bool wait_progress(const int* counter, int need, int* seen, DevStatus* st, long long spin,
+                                              int where) {
+  long long polls = 0;
+  int v = ld_acquire_s32(counter);
+  while (v < need) {
+    if (++polls > spin) { dev_fail(st, LU_ERR_TIMEOUT, where); return false; }
+    if ((polls & 255) == 0 && ld_acquire_s32(&st->code) != 0) return false;
+    const int gap = need - v;
+    if (gap > 2) __nanosleep(min(gap, 64) * 256);
+    v = ld_acquire_s32(counter);
+  }
+  *seen = v;
+  return true;
+}
+
 // TS: storage type of the factors; T: type of the vector and the arithmetic
 // (FP32 factors with an FP64 vector give the GMRES-IR preconditioner solve
 // in working precision at the FP32 factors' memory cost).
+// Dynamic shared memory: inverse of the diagonal tile (T, [TB][TB + 1]),
+// then the tile as stored (TS, [TB][TB + 1]).
+template <typename TS, typename T>
+__host__ __device__ constexpr size_t trsv_smem() {
+  return (size_t)TB * (TB + 1) * (sizeof(T) + sizeof(TS));
+}
+
 template <typename TS, typename T, bool UPPER>
 __global__ void __launch_bounds__(256) trsv_kernel(const TS* LU, int64_t lda, int n, T* x, int* flags,
                                                    unsigned* ticket, DevStatus* st, long long spin) {
-  __shared__ T sD[TB][TB + 1];
+  extern __shared__ __align__(16) unsigned char trsv_raw[];
+  T* sInv = reinterpret_cast<T*>(trsv_raw);
+  TS* sD = reinterpret_cast<TS*>(sInv + TB * (TB + 1));
   __shared__ T s_acc[TB];
+  __shared__ T s_rhs[TB];
   __shared__ int s_blk;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) s_blk = (int)atomicAdd(ticket, 1u);
@@ -64,44 +133,61 @@ __global__ void __launch_bounds__(256) trsv_kernel(const TS* LU, int64_t lda, in
   const int bi = UPPER ? nblk - 1 - tk : tk;
   const int r0 = bi * TB, rows = min(TB, n - r0);
 
-  for (int idx = tid; idx < TB * TB; idx += blockDim.x) {
-    const int i = idx / TB, j = idx - i * TB;
-    sD[i][j] = (i < rows && j < rows) ? (T)LU[(int64_t)(r0 + i) * lda + r0 + j] : T(0);
+  // off the chain: this block's right-hand side, the diagonal tile and its
+  // inverse (no other CTA writes these rows of x before this one does)
+  const T own = tid < rows ? x[r0 + tid] : T(0);
+#pragma unroll 4
+  for (int u = 0; u < TB * TB / 256; u++) {
+    const int idx = tid + u * 256;
+    const int i = idx / TB, jj = idx - i * TB;
+    sD[i * (TB + 1) + jj] = (i < rows && jj < rows) ? LU[(int64_t)(r0 + i) * lda + r0 + jj] : TS(0);
   }
+  __syncthreads();
+  tri_inverse_tile<UPPER, TS, T>(sD, TB + 1, sInv, TB + 1, rows);
 
   T acc[8];
 #pragma unroll
   for (int i = 0; i < 8; i++) acc[i] = T(0);
   const int nvisit = UPPER ? (nblk - 1 - bi) : bi;
   bool ok = true;
-  for (int q = 0; q < nvisit && ok; q++) {
-    const int cb = UPPER ? nblk - 1 - q : q;
-    const int c0 = cb * TB;
-    T lv[8][2];
+  // this warp's 8 rows of tile q (registers): the next tile's loads are in
+  // flight while the warp waits for the current block
+  auto load_tile = [&](int q, TS (&dst)[8][2]) {
+    const int c0 = (UPPER ? nblk - 1 - q : q) * TB;
 #pragma unroll
     for (int i = 0; i < 8; i++) {
       const int r = r0 + warp * 8 + i;
 #pragma unroll
       for (int e = 0; e < 2; e++) {
         const int c = c0 + lane * 2 + e;
-        lv[i][e] = (r < n && c < n) ? (T)__ldcs(&LU[(int64_t)r * lda + c]) : T(0);
+        dst[i][e] = (r < n && c < n) ? __ldcs(&LU[(int64_t)r * lda + c]) : TS(0);
       }
     }
-    if (lane == 0) {
-      long long polls = 0;
-      while (ld_acquire_s32(&flags[cb]) == 0) {
-        if (++polls > spin) { dev_fail(st, LU_ERR_TIMEOUT, 301); ok = false; break; }
-        if ((polls & 1023) == 0 && ld_acquire_s32(&st->code) != 0) { ok = false; break; }
-      }
+  };
+  TS lv[8][2], lvn[8][2];
+  if (nvisit > 0) load_tile(0, lv);
+  int seen = 0;
+  for (int q = 0; q < nvisit && ok; q++) {
+    const int cb = UPPER ? nblk - 1 - q : q;
+    const int c0 = cb * TB;
+    if (q + 1 < nvisit) load_tile(q + 1, lvn);
+    if (q + 1 > seen) {  // block q (in ticket order) not known to be final yet
+      int v = 0;
+      if (lane == 0) ok = wait_progress(&flags[0], q + 1, &v, st, spin, 301);
+      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+      seen = __shfl_sync(0xffffffffu, v, 0);
+      if (!ok) break;
     }
-    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-    __syncwarp();
-    if (!ok) break;
     const int c = c0 + lane * 2;
     const T x0 = c < n ? __ldcg(&x[c]) : T(0);
     const T x1 = c + 1 < n ? __ldcg(&x[c + 1]) : T(0);
 #pragma unroll
-    for (int i = 0; i < 8; i++) acc[i] = fma(lv[i][1], x1, fma(lv[i][0], x0, acc[i]));
+    for (int i = 0; i < 8; i++) acc[i] = fma((T)lv[i][1], x1, fma((T)lv[i][0], x0, acc[i]));
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      lv[i][0] = lvn[i][0];
+      lv[i][1] = lvn[i][1];
+    }
   }
 #pragma unroll
   for (int i = 0; i < 8; i++) {
@@ -110,56 +196,85 @@ __global__ void __launch_bounds__(256) trsv_kernel(const TS* LU, int64_t lda, in
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) s_acc[warp * 8 + i] = v;
   }
+  if (!__syncthreads_and(ok ? 1 : 0)) return;
+  if (tid < TB) s_rhs[tid] = own - s_acc[tid];
   __syncthreads();
-  if (!ok) return;
-  if (warp == 0) {
-    T v0 = lane < rows ? x[r0 + lane] - s_acc[lane] : T(0);
-    T v1 = lane + 32 < rows ? x[r0 + lane + 32] - s_acc[lane + 32] : T(0);
-    if (!UPPER) {
-      for (int j = 0; j < rows; j++) {
-        const T xj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-        if (lane > j) v0 = fma(-sD[lane][j], xj, v0);
-        if (lane + 32 > j) v1 = fma(-sD[lane + 32][j], xj, v1);
-      }
-    } else {
-      for (int j = rows - 1; j >= 0; j--) {
-        // owner finalises x_j, then broadcasts
-        if (j < 32) { if (lane == j) v0 = v0 / sD[j][j]; }
-        else        { if (lane == j - 32) v1 = v1 / sD[j][j]; }
-        const T xj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-        if (lane < j) v0 = fma(-sD[lane][j], xj, v0);
-        if (lane + 32 < j) v1 = fma(-sD[lane + 32][j], xj, v1);
-      }
+  // x_bi = Dinv (b_bi - off-diagonal part): row tid / 4, a quarter of the columns
+  {
+    const int r = tid >> 2, q4 = tid & 3;
+    T sum = T(0);
+#pragma unroll
+    for (int m = 0; m < TB / 4; m++) {
+      const int cc = q4 + 4 * m;
+      sum = fma(sInv[r * (TB + 1) + cc], s_rhs[cc], sum);
     }
-    if (lane < rows) x[r0 + lane] = v0;
-    if (lane + 32 < rows) x[r0 + lane + 32] = v1;
-    __threadfence();
-    __syncwarp();
-    if (lane == 0) st_release_s32(&flags[bi], 1);
+    sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+    sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+    if (q4 == 0 && r < rows) x[r0 + r] = sum;
   }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) st_release_s32(&flags[0], tk + 1);
 }
 
 // ---------------------------------------------------------------------------
 // Multi-right-hand-side triangular solve T Y = B in place on a row-major
-// n x nrhs block (nrhs <= 16 per launch), T taken from row-major LU factors:
+// n x nrhs FP64 block (nrhs <= 16 per launch), T taken from row-major LU
+// factors stored as TS (FP64, or FP32 factors applied in FP64 arithmetic):
 //   MODE 0  LN: T = L  (unit lower)      forward,  tiles L[bi][bk], bk < bi
 //   MODE 1  UN: T = U  (upper)           backward, tiles U[bi][bk], bk > bi
 //   MODE 2  UT: T = U^T (lower)          forward,  tiles U[bk][bi]^T, bk < bi
 //   MODE 3  LT: T = L^T (unit upper)     backward, tiles L[bk][bi]^T, bk > bi
 // Modes 2 and 3 are the transposed solves of the adjoint (A^T lambda = W).
-// Same ticket/flag pipeline as trsv_kernel; every 64 x 64 tile is staged in
-// shared memory with coalesced row reads, so the transposed modes read the
-// factor by rows too.
+// Same ticket / progress-counter pipeline as trsv_kernel, with the inverted
+// diagonal tile.  Both 64 x 64 x 16 products of a step (an off-diagonal
+// tile against the finished rows of Y, and the inverted diagonal tile
+// against the block's right-hand side) run on the FP64 tensor pipe
+// (mma.sync m16n8k4; warp w owns output rows 16 (w / 2).., columns
+// 8 (w % 2)..).  The factor tiles do not depend on the pipeline, so they
+// stream through a two-stage cp.async ring (tile q+1 in flight while the
+// CTA waits for block q and applies tile q); only the 64 x 16 slice of Y
+// waits for the counter.  Tiles are read by rows in every mode (the
+// transposed modes index the staged tile transposed).  Pitches keep the
+// fragment loads free of bank conflicts.
+// Dynamic shared memory: the ring, then the FP64 inverse of the diagonal
+// tile ([TB][kInvPitch], D^{-1} of the stored tile).
 // ---------------------------------------------------------------------------
-template <int MODE>
-__global__ void __launch_bounds__(256) trsm_pipe_kernel(const double* LU, int64_t lda, int n, double* Y, int64_t ldy,
+template <typename TS, bool TRANS>
+__host__ __device__ constexpr int pipe_pitch() { return (sizeof(TS) == 4 && TRANS) ? 72 : 68; }
+template <typename TS>
+__host__ __device__ constexpr size_t pipe_ring_bytes() {
+  return 2 * (size_t)TB * (pipe_pitch<TS, false>() > pipe_pitch<TS, true>() ? pipe_pitch<TS, false>()
+                                                                            : pipe_pitch<TS, true>()) *
+         sizeof(TS);
+}
+constexpr int kInvPitch = 68;
+constexpr int kYkPitch = 20;
+template <typename TS>
+__host__ __device__ constexpr size_t pipe_smem() {
+  return pipe_ring_bytes<TS>() + (size_t)TB * kInvPitch * sizeof(double);
+}
+
+__device__ __forceinline__ void dmma16x8x4(double (&c)[4], double a0, double a1, double b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+
+template <typename TS, int MODE>
+__global__ void __launch_bounds__(256, 2) trsm_pipe_kernel(const TS* LU, int64_t lda, int n, double* Y, int64_t ldy,
                                                         int nrhs, int* flags, unsigned* ticket, DevStatus* st,
                                                         long long spin) {
   constexpr bool FWD = (MODE == 0 || MODE == 2);
   constexpr bool TRANS = (MODE >= 2);
-  constexpr bool UNIT = (MODE == 0 || MODE == 3);
-  __shared__ double tile[TB][TB + 1];
-  __shared__ double yk[TB][17];
+  constexpr int TP = pipe_pitch<TS, TRANS>();
+  constexpr int EPC = 16 / (int)sizeof(TS);   // elements per 16-byte chunk
+  constexpr int CPR = TB / EPC;               // chunks per tile row
+  extern __shared__ __align__(16) unsigned char pipe_raw[];
+  TS* ring = reinterpret_cast<TS*>(pipe_raw);  // [2][TB][TP]
+  double* dinv = reinterpret_cast<double*>(pipe_raw + pipe_ring_bytes<TS>());  // [TB][kInvPitch]
+  __shared__ __align__(16) double yk[TB][kYkPitch];
   __shared__ int s_blk, s_ok;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) s_blk = (int)atomicAdd(ticket, 1u);
@@ -169,92 +284,107 @@ __global__ void __launch_bounds__(256) trsm_pipe_kernel(const double* LU, int64_
   if (tk >= nblk) return;
   const int bi = FWD ? tk : nblk - 1 - tk;
   const int r0 = bi * TB, rows = min(TB, n - r0);
-  // this thread's outputs: row r = tid / 4, rhs columns 4*(tid%4) .. +3
-  const int orow = tid >> 2, oc = (tid & 3) * 4;
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
   const int nvisit = FWD ? bi : nblk - 1 - bi;
+  // MMA fragment coordinates: group g, thread-in-group t; warp tile rows
+  // m0 .. m0 + 15, columns n0 .. n0 + 7
+  const int g = lane >> 2, t = lane & 3;
+  const int m0 = (warp >> 1) * 16, n0 = (warp & 1) * 8;
+
+  // stage a tile into ring slot `slot`: rows grow0.., cols gcol0.. (nrow x ncol valid)
+  auto stage = [&](int slot, int grow0, int gcol0, int nrow, int ncol) {
+    TS* buf = ring + slot * TB * TP;
+    for (int ch = tid; ch < TB * CPR; ch += 256) {
+      const int i = ch / CPR, j = (ch - i * CPR) * EPC;
+      const int valid = i < nrow ? max(0, min(EPC, ncol - j)) : 0;
+      const TS* src = valid ? LU + (int64_t)(grow0 + i) * lda + gcol0 + j : LU;
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(buf + i * TP + j)), "l"(src),
+                   "r"(valid * (int)sizeof(TS))
+                   : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  // off-diagonal tile q: NoTrans rows r0.., cols c0..; Trans rows c0.., cols r0..
+  auto issue = [&](int q) {
+    const int c0 = (FWD ? q : nblk - 1 - q) * TB, cw = min(TB, n - c0);
+    if (TRANS) stage(q & 1, c0, r0, cw, rows);
+    else stage(q & 1, r0, c0, rows, cw);
+  };
+
+  // off the chain: this block's right-hand side (in the accumulator layout),
+  // the diagonal tile through ring slot 0 and its inverse
+  double own[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const int r = m0 + g + (e >> 1) * 8, c = n0 + 2 * t + (e & 1);
+    own[e] = (r < rows && c < nrhs) ? Y[(int64_t)(r0 + r) * ldy + c] : 0.0;
+  }
+  stage(0, r0, r0, rows, rows);
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  __syncthreads();
+  // D^{-1} of the stored tile (U for modes 1 and 2, unit L for 0 and 3);
+  // T^{-1} is D^{-1} or its transpose
+  tri_inverse_tile<(MODE == 1 || MODE == 2), TS, double>(ring, TP, dinv, kInvPitch, rows);
+  __syncthreads();  // ring slot 0 is reused below
+
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
   bool ok = true;
+  int seen = 0;
+  if (nvisit > 0) issue(0);
   for (int q = 0; q < nvisit; q++) {
     const int bk = FWD ? q : nblk - 1 - q;
     const int c0 = bk * TB, cw = min(TB, n - c0);
-    // stage the tile: NoTrans T[bi][bk] rows r0.., cols c0..; Trans: rows c0.., cols r0..
-    for (int idx = tid; idx < TB * TB; idx += blockDim.x) {
-      const int i = idx / TB, j = idx - i * TB;
-      double v = 0.0;
-      if (!TRANS) {
-        if (i < rows && j < cw) v = __ldcs(&LU[(int64_t)(r0 + i) * lda + c0 + j]);
-      } else {
-        if (i < cw && j < rows) v = __ldcs(&LU[(int64_t)(c0 + i) * lda + r0 + j]);
+    if (q + 1 < nvisit) issue(q + 1);
+    if (q + 1 > seen) {  // block q (in ticket order) not known to be final yet
+      if (tid == 0) {
+        int v = 0;
+        s_ok = wait_progress(&flags[0], q + 1, &v, st, spin, 302) ? v : -1;
       }
-      tile[i][j] = v;
+      __syncthreads();
+      seen = s_ok;
+      if (seen < 0) { ok = false; break; }
     }
-    if (tid == 0) {
-      long long polls = 0;
-      s_ok = 1;
-      while (ld_acquire_s32(&flags[bk]) == 0) {
-        if (++polls > spin) { dev_fail(st, LU_ERR_TIMEOUT, 302); s_ok = 0; break; }
-        if ((polls & 1023) == 0 && ld_acquire_s32(&st->code) != 0) { s_ok = 0; break; }
-      }
-    }
-    __syncthreads();
-    if (!s_ok) { ok = false; break; }
-    for (int idx = tid; idx < TB * 16; idx += blockDim.x) {
+#pragma unroll
+    for (int u = 0; u < TB * 16 / 256; u++) {
+      const int idx = tid + u * 256;
       const int i = idx >> 4, c = idx & 15;
       yk[i][c] = (i < cw && c < nrhs) ? __ldcg(&Y[(int64_t)(c0 + i) * ldy + c]) : 0.0;
     }
+    if (q + 1 < nvisit) asm volatile("cp.async.wait_group 1;" ::: "memory");
+    else asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncthreads();
-#pragma unroll 4
-    for (int k = 0; k < TB; k++) {
-      const double t = TRANS ? tile[k][orow] : tile[orow][k];
+    const TS* tq = ring + (q & 1) * TB * TP;
+    // acc += T[bi][bk] * Y[bk] on this warp's 16 x 8 tile
 #pragma unroll
-      for (int e = 0; e < 4; e++) acc[e] = fma(t, yk[k][oc + e], acc[e]);
+    for (int ks = 0; ks < TB / 4; ks++) {
+      const int k = ks * 4 + t;
+      const double a0 = (double)(TRANS ? tq[k * TP + m0 + g] : tq[(m0 + g) * TP + k]);
+      const double a1 = (double)(TRANS ? tq[k * TP + m0 + g + 8] : tq[(m0 + g + 8) * TP + k]);
+      dmma16x8x4(acc, a0, a1, yk[k][n0 + g]);
     }
-    __syncthreads();
+    __syncthreads();  // ring slot, yk and s_ok are rewritten next
   }
-  if (!ok) return;
-  // right-hand side minus the off-diagonal contributions, then the diagonal tile
-  for (int e = 0; e < 4; e++) {
-    const int c = oc + e;
-    yk[orow][c] = (orow < rows && c < nrhs) ? Y[(int64_t)(r0 + orow) * ldy + c] - acc[e] : 0.0;
-  }
-  for (int idx = tid; idx < TB * TB; idx += blockDim.x) {
-    const int i = idx / TB, j = idx - i * TB;
-    // diagonal tile in the orientation of T: T(i, j)
-    double v = 0.0;
-    if (i < rows && j < rows) v = TRANS ? LU[(int64_t)(r0 + j) * lda + r0 + i] : LU[(int64_t)(r0 + i) * lda + r0 + j];
-    tile[i][j] = v;
-  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  if (!ok) return;  // uniform: every thread read the same s_ok
+  // R = B_bi - off-diagonal part (into yk), then Y_bi = T^{-1} R
+#pragma unroll
+  for (int e = 0; e < 4; e++) yk[m0 + g + (e >> 1) * 8][n0 + 2 * t + (e & 1)] = own[e] - acc[e];
   __syncthreads();
-  // warp w solves rhs columns w and w + 8; lanes own rows lane and lane + 32
-  for (int c = warp; c < nrhs; c += 8) {
-    double v0 = yk[lane][c], v1 = yk[lane + 32][c];
-    if (FWD) {
-      for (int j = 0; j < rows; j++) {
-        if (!UNIT) {
-          if (j < 32) { if (lane == j) v0 = v0 / tile[j][j]; }
-          else        { if (lane == j - 32) v1 = v1 / tile[j][j]; }
-        }
-        const double xj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-        if (lane > j) v0 = fma(-tile[lane][j], xj, v0);
-        if (lane + 32 > j) v1 = fma(-tile[lane + 32][j], xj, v1);
-      }
-    } else {
-      for (int j = rows - 1; j >= 0; j--) {
-        if (!UNIT) {
-          if (j < 32) { if (lane == j) v0 = v0 / tile[j][j]; }
-          else        { if (lane == j - 32) v1 = v1 / tile[j][j]; }
-        }
-        const double xj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-        if (lane < j) v0 = fma(-tile[lane][j], xj, v0);
-        if (lane + 32 < j) v1 = fma(-tile[lane + 32][j], xj, v1);
-      }
-    }
-    if (lane < rows) Y[(int64_t)(r0 + lane) * ldy + c] = v0;
-    if (lane + 32 < rows) Y[(int64_t)(r0 + lane + 32) * ldy + c] = v1;
+  double out[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int ks = 0; ks < TB / 4; ks++) {
+    const int k = ks * 4 + t;
+    const double a0 = TRANS ? dinv[k * kInvPitch + m0 + g] : dinv[(m0 + g) * kInvPitch + k];
+    const double a1 = TRANS ? dinv[k * kInvPitch + m0 + g + 8] : dinv[(m0 + g + 8) * kInvPitch + k];
+    dmma16x8x4(out, a0, a1, yk[k][n0 + g]);
+  }
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const int r = m0 + g + (e >> 1) * 8, c = n0 + 2 * t + (e & 1);
+    if (r < rows && c < nrhs) Y[(int64_t)(r0 + r) * ldy + c] = out[e];
   }
   __threadfence();
   __syncthreads();
-  if (tid == 0) st_release_s32(&flags[bi], 1);
+  if (tid == 0) st_release_s32(&flags[0], tk + 1);
 }
 
 // G = -Lam * X^T (n x n), Lam and X n x k row-major, k <= 16: the rank-k
@@ -299,19 +429,38 @@ __global__ void permute_rows_kernel(const double* X, int64_t ldx, double* Y, int
 
 }  // namespace
 
-int launch_trsm_pipe(const double* LU, int64_t lda, int n, double* Y, int64_t ldy, int nrhs, int mode, int* flags,
+template <typename TS, int MODE>
+int pipe_attr() {
+  static bool done = false;
+  if (!done) {
+    LUB_CUDA(cudaFuncSetAttribute(trsm_pipe_kernel<TS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)pipe_smem<TS>()));
+    done = true;
+  }
+  return LU_OK;
+}
+
+template <typename TS>
+int launch_trsm_pipe(const TS* LU, int64_t lda, int n, double* Y, int64_t ldy, int nrhs, int mode, int* flags,
                      unsigned* ticket, DevStatus* st, long long spin, cudaStream_t s) {
   if (n <= 0 || nrhs <= 0) return LU_OK;
+  // factor rows are staged in 16-byte chunks
+  if (((lda * (int64_t)sizeof(TS)) & 15) || (reinterpret_cast<uintptr_t>(LU) & 15)) return LU_ERR_ALIGN;
+  LUB_TRY((pipe_attr<TS, 0>()));
+  LUB_TRY((pipe_attr<TS, 1>()));
+  LUB_TRY((pipe_attr<TS, 2>()));
+  LUB_TRY((pipe_attr<TS, 3>()));
+  const size_t smem = pipe_smem<TS>();
   const int nblk = ceil_div(n, TB);
   for (int c0 = 0; c0 < nrhs; c0 += 16) {
     const int k = std::min(16, nrhs - c0);
-    LUB_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * nblk, s));
+    LUB_CUDA(cudaMemsetAsync(flags, 0, sizeof(int), s));  // progress counter
     LUB_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), s));
     switch (mode) {
-      case 0: trsm_pipe_kernel<0><<<nblk, 256, 0, s>>>(LU, lda, n, Y + c0, ldy, k, flags, ticket, st, spin); break;
-      case 1: trsm_pipe_kernel<1><<<nblk, 256, 0, s>>>(LU, lda, n, Y + c0, ldy, k, flags, ticket, st, spin); break;
-      case 2: trsm_pipe_kernel<2><<<nblk, 256, 0, s>>>(LU, lda, n, Y + c0, ldy, k, flags, ticket, st, spin); break;
-      case 3: trsm_pipe_kernel<3><<<nblk, 256, 0, s>>>(LU, lda, n, Y + c0, ldy, k, flags, ticket, st, spin); break;
+      case 0: trsm_pipe_kernel<TS, 0><<<nblk, 256, smem, s>>>(LU, lda, n, Y + c0, ldy, k, flags, ticket, st, spin); break;
+      case 1: trsm_pipe_kernel<TS, 1><<<nblk, 256, smem, s>>>(LU, lda, n, Y + c0, ldy, k, flags, ticket, st, spin); break;
+      case 2: trsm_pipe_kernel<TS, 2><<<nblk, 256, smem, s>>>(LU, lda, n, Y + c0, ldy, k, flags, ticket, st, spin); break;
+      case 3: trsm_pipe_kernel<TS, 3><<<nblk, 256, smem, s>>>(LU, lda, n, Y + c0, ldy, k, flags, ticket, st, spin); break;
       default: return LU_ERR_ARG;
     }
     LUB_LAUNCH_CHECK();
@@ -353,12 +502,20 @@ int launch_trsv_mixed(const TS* LU, int64_t lda, int n, T* x, int upper, int* fl
                       long long spin, cudaStream_t s) {
   if (n <= 0) return LU_OK;
   const int nblk = ceil_div(n, TB);
-  LUB_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * nblk, s));
+  constexpr size_t smem = trsv_smem<TS, T>();
+  static bool attr = false;
+  if (!attr) {
+    LUB_CUDA(cudaFuncSetAttribute(trsv_kernel<TS, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LUB_CUDA(cudaFuncSetAttribute(trsv_kernel<TS, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = true;
+  }
+  // flags[0] is the progress counter; the ticket hands out block order
+  LUB_CUDA(cudaMemsetAsync(flags, 0, sizeof(int), s));
   LUB_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), s));
   if (upper)
-    trsv_kernel<TS, T, true><<<nblk, 256, 0, s>>>(LU, lda, n, x, flags, ticket, st, spin);
+    trsv_kernel<TS, T, true><<<nblk, 256, smem, s>>>(LU, lda, n, x, flags, ticket, st, spin);
   else
-    trsv_kernel<TS, T, false><<<nblk, 256, 0, s>>>(LU, lda, n, x, flags, ticket, st, spin);
+    trsv_kernel<TS, T, false><<<nblk, 256, smem, s>>>(LU, lda, n, x, flags, ticket, st, spin);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }
@@ -371,6 +528,10 @@ int launch_trsv(const T* LU, int64_t lda, int n, T* x, int upper, int* flags, un
 template int launch_trsv_mixed<float, double>(const float*, int64_t, int, double*, int, int*, unsigned*, DevStatus*,
                                               long long, cudaStream_t);
 
+template int launch_trsm_pipe<double>(const double*, int64_t, int, double*, int64_t, int, int, int*, unsigned*,
+                                      DevStatus*, long long, cudaStream_t);
+template int launch_trsm_pipe<float>(const float*, int64_t, int, double*, int64_t, int, int, int*, unsigned*,
+                                     DevStatus*, long long, cudaStream_t);
 template int launch_trsm_llu_leaf<double>(const double*, int64_t, double*, int64_t, int, int, cudaStream_t);
 template int launch_trsm_llu_leaf<float>(const float*, int64_t, float*, int64_t, int, int, cudaStream_t);
 template int launch_trsv<double>(const double*, int64_t, int, double*, int, int*, unsigned*, DevStatus*, long long,

@@ -159,6 +159,42 @@ LU_API int lu_residual(lu_handle h, const double* dA, int64_t lda, const double*
 LU_API int lu_refine_solve(lu_handle h, const double* dA, int64_t lda, const double* db, double* dx,
                     lu_refine_info* info, void* stream);
 
+/* Low-precision factorisation kept in the handle (no reference
+ * counterpart): dA (read only) is converted to FP32 and factored as in
+ * lu_refine_solve (cfg.precision: BF16, scaled FP16 or FP16x3 trailing
+ * updates); the FP32 factors and their row permutation stay in the handle
+ * for lu_refine_apply / lu_refine_adjoint until the next lu_refine_factor or
+ * lu_refine_solve on it.  Asynchronous; a singular pivot is reported by the
+ * next lu_refine_apply (info->status) and by lu_status. */
+LU_API int lu_refine_factor(lu_handle h, const double* dA, int64_t lda, void* stream);
+
+/* op(A) X = B with op(A) = A (trans = 0) or A^T (trans = 1) for nrhs
+ * columns, by FP64 iterative refinement on the factors of the last
+ * lu_refine_factor (no reference counterpart).  dA must be the matrix those
+ * factors came from (FP64, even lda, 16-byte aligned): every step computes
+ * the FP64 residual R = B - op(A) X and corrects X through the FP32 factors,
+ * until each column's scaled residual
+ *   ||r||inf / ((||op(A)||inf ||x||inf + ||b||inf) n eps)
+ * is below cfg.ir_target (16 when 0) or cfg.ir_max_iter steps (50 when 0)
+ * have run.  When classical steps stop contracting (or cfg.ir_mode is
+ * LU_IR_GMRES), the columns still above the target get GMRES-IR cycles
+ * (restart 120, FP32 factors as the preconditioner).  dB (n x nrhs, ldb) is
+ * read only; dX receives X.  info reports the worst column; status
+ * LU_ERR_NOCONV when a column did not converge.  Synchronises the stream
+ * once per refinement step. */
+LU_API int lu_refine_apply(lu_handle h, const double* dA, int64_t lda, int trans, const double* dB,
+                    int64_t ldb, double* dX, int64_t ldx, int64_t nrhs, lu_refine_info* info,
+                    void* stream);
+
+/* Adjoint of X = A^{-1} B on low-precision factors (no reference
+ * counterpart): lambda = A^{-T} W by lu_refine_apply (trans = 1) into
+ * gradB, then grad_A = -lambda X^T into gradA (n x n, ldga; may be NULL).
+ * Needs the factors of dA from lu_refine_factor. */
+LU_API int lu_refine_adjoint(lu_handle h, const double* dA, int64_t lda, const double* dX,
+                      int64_t ldx, const double* dW, int64_t ldw, int64_t nrhs, double* gradB,
+                      int64_t ldgb, double* gradA, int64_t ldga, lu_refine_info* info,
+                      void* stream);
+
 /* Adjoint of X = A^{-1} B (no reference counterpart).  Given the factors
  * of A (from lu_factor), X (n x nrhs) and the upstream gradient W = dL/dX,
  * computes lambda = A^{-T} W into gradB and grad_A = -lambda X^T into gradA
