@@ -57,6 +57,7 @@ struct lu_handle_s {
   int gemm_ctas = 148, gemm_reserve = 48;
   int32_t* perm = nullptr;
   int32_t* perm_work = nullptr;
+  int32_t* perm_lists = nullptr;  // composed pivot batches (ipiv -> perm)
   int* trsv_flags = nullptr;
   unsigned* trsv_ticket = nullptr;
   double* vec = nullptr;

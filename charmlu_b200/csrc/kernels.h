@@ -61,6 +61,8 @@ int launch_pivot_apply(T* A, int64_t lda, int c_begin, int c_end, int skip_begin
 // x <- P x in place from an ipiv vector (single CTA, shared memory only).
 int launch_ipiv_apply_vector(const int32_t* ipiv, int n, double* x, cudaStream_t s);
 // Full permutation from an ipiv vector (single CTA, batched composition).
+// work: ipiv_to_perm_work_ints(n) ints
+int ipiv_to_perm_work_ints(int n);
 int launch_ipiv_to_perm(const int32_t* ipiv, int n, int32_t* perm, int32_t* work, cudaStream_t s);
 
 // ---- triangular solves

@@ -325,6 +325,7 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
   if (const char* e = getenv("LU_B200_GEMM_RESERVE")) h->gemm_reserve = std::max(0, atoi(e));
   if (s == LU_OK) s = h->alloc(&h->perm, n);
   if (s == LU_OK) s = h->alloc(&h->perm_work, n);
+  if (s == LU_OK) s = h->alloc(&h->perm_lists, lub::ipiv_to_perm_work_ints((int)n));
   if (s == LU_OK) s = h->alloc(&h->trsv_flags, n / 64 + 2);
   if (s == LU_OK) s = h->alloc(&h->trsv_ticket, 1);
   if (s == LU_OK) s = h->alloc(&h->vec, n);
@@ -406,7 +407,7 @@ int lu_solve(lu_handle h, const double* dLU, int64_t lda, const int32_t* ipiv, d
   if (!ipiv || !dB || nrhs < 1 || ldb < nrhs || (trans != 0 && trans != 1)) return LU_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   const int n = (int)h->cfg.n;
-  LUB_TRY(launch_ipiv_to_perm(ipiv, n, h->perm_work, nullptr, s));
+  LUB_TRY(launch_ipiv_to_perm(ipiv, n, h->perm_work, h->perm_lists, s));
   if (trans == 0 && nrhs == 1) {
     LUB_TRY(launch_gather_perm(dB, h->perm_work, h->vec, n, s));
     LUB_TRY(solve_permuted_f64(h, dLU, lda, h->vec, s));
@@ -473,7 +474,7 @@ int lu_adjoint(lu_handle h, const double* dLU, int64_t lda, const int32_t* ipiv,
   if (!ipiv || !dW || !gradB || nrhs < 1 || ldw < nrhs || ldgb < nrhs) return LU_ERR_ARG;
   if (gradA && (!dX || ldx < nrhs || ldga < n)) return LU_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
-  LUB_TRY(launch_ipiv_to_perm(ipiv, (int)n, h->perm_work, nullptr, s));
+  LUB_TRY(launch_ipiv_to_perm(ipiv, (int)n, h->perm_work, h->perm_lists, s));
   LUB_TRY(solve_trans_multi(h, dLU, lda, dW, ldw, (int)nrhs, gradB, ldgb, s));
   if (gradA) {
     Prof pf(h, s, LU_PH_OTHER, 2.0 * n * (double)n * nrhs);

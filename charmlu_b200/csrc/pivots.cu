@@ -86,30 +86,73 @@ __global__ void __launch_bounds__(1024) pivot_compose_kernel(const int32_t* ipiv
   if (threadIdx.x == 0) *pl.m = m;
 }
 
-template <typename T, int CS>
-__global__ void __launch_bounds__(256) pivot_apply_kernel(T* A, int64_t lda, int c_begin, int c_end, int skip_begin,
-                                                          int skip_end, PivotList pl, double* rhs, int32_t* perm) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* buf = reinterpret_cast<T*>(smem_raw);
+// One CTA per 128-byte column strip: every moved row's segment of the strip
+// is read into registers (16-byte chunks, eight per thread, all loads in
+// flight together), then, after one barrier, written to its destination.
+// Chunks that straddle the strip's valid column range (or rows that are not
+// 16-byte aligned, vec_ok = 0) go element by element.
+constexpr int kApplyThreads = 1024;
+constexpr int kApplyUnroll = 8;  // chunks per thread: 1024 rows x 8 chunks per strip
+
+template <typename T>
+__device__ __forceinline__ bool col_live(int cc, int c_begin, int c_end, int skip_begin, int skip_end) {
+  return cc >= c_begin && cc < c_end && (cc < skip_begin || cc >= skip_end);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kApplyThreads) pivot_apply_kernel(T* A, int64_t lda, int c_begin, int c_end,
+                                                                   int skip_begin, int skip_end, PivotList pl,
+                                                                   double* rhs, int32_t* perm, int vec_ok) {
+  constexpr int EPC = 16 / (int)sizeof(T);  // elements per chunk
+  constexpr int CS = 8 * EPC;               // elements per strip
+  __shared__ double vb[2 * kMaxBatch];
+  __shared__ int32_t pb[2 * kMaxBatch];
   const int m = *pl.m;
   const int tid = threadIdx.x;
   const int c0 = c_begin + blockIdx.x * CS;
   const bool strip_live = c0 < c_end && !(c0 >= skip_begin && c0 + CS <= skip_end);
   if (strip_live && m > 0) {
-    for (int idx = tid; idx < m * CS; idx += blockDim.x) {
-      const int i = idx / CS, c = idx - i * CS, col = c0 + c;
-      if (col < c_end && (col < skip_begin || col >= skip_end)) buf[idx] = A[(int64_t)pl.src[i] * lda + col];
+    uint4 v[kApplyUnroll];
+#pragma unroll
+    for (int u = 0; u < kApplyUnroll; u++) {
+      const int pr = tid + u * kApplyThreads;
+      const int i = pr >> 3, col = c0 + (pr & 7) * EPC;
+      if (i < m) {
+        const T* src = A + (int64_t)pl.src[i] * lda + col;
+        if (vec_ok && col_live<T>(col, c_begin, c_end, skip_begin, skip_end) &&
+            col_live<T>(col + EPC - 1, c_begin, c_end, skip_begin, skip_end)) {
+          v[u] = __ldcs(reinterpret_cast<const uint4*>(src));
+        } else {
+          T tmp[EPC];
+#pragma unroll
+          for (int e = 0; e < EPC; e++)
+            tmp[e] = col_live<T>(col + e, c_begin, c_end, skip_begin, skip_end) ? src[e] : T(0);
+          memcpy(&v[u], tmp, 16);
+        }
+      }
     }
-    __syncthreads();
-    for (int idx = tid; idx < m * CS; idx += blockDim.x) {
-      const int i = idx / CS, c = idx - i * CS, col = c0 + c;
-      if (col < c_end && (col < skip_begin || col >= skip_end)) A[(int64_t)pl.dst[i] * lda + col] = buf[idx];
+    __syncthreads();  // every source segment of the strip is in registers
+#pragma unroll
+    for (int u = 0; u < kApplyUnroll; u++) {
+      const int pr = tid + u * kApplyThreads;
+      const int i = pr >> 3, col = c0 + (pr & 7) * EPC;
+      if (i < m) {
+        T* dst = A + (int64_t)pl.dst[i] * lda + col;
+        if (vec_ok && col_live<T>(col, c_begin, c_end, skip_begin, skip_end) &&
+            col_live<T>(col + EPC - 1, c_begin, c_end, skip_begin, skip_end)) {
+          __stcs(reinterpret_cast<uint4*>(dst), v[u]);
+        } else {
+          T tmp[EPC];
+          memcpy(tmp, &v[u], 16);
+#pragma unroll
+          for (int e = 0; e < EPC; e++)
+            if (col_live<T>(col + e, c_begin, c_end, skip_begin, skip_end)) dst[e] = tmp[e];
+        }
+      }
     }
   }
   if (blockIdx.x == 0 && m > 0 && (rhs || perm)) {
     __syncthreads();
-    double* vb = reinterpret_cast<double*>(smem_raw);
-    int32_t* pb = reinterpret_cast<int32_t*>(vb + m);
     for (int i = tid; i < m; i += blockDim.x) {
       if (rhs) vb[i] = rhs[pl.src[i]];
       if (perm) pb[i] = perm[pl.src[i]];
@@ -122,20 +165,38 @@ __global__ void __launch_bounds__(256) pivot_apply_kernel(T* A, int64_t lda, int
   }
 }
 
-// perm <- iota, then all pivot batches of 256 composed and applied in order.
-__global__ void __launch_bounds__(1024) ipiv_to_perm_kernel(const int32_t* ipiv, int n, int32_t* perm, int32_t* work) {
-  __shared__ int p[256], nxt[256], lb[256];
-  __shared__ int dst[512], src[512];
-  __shared__ int vals[512];
+// ipiv -> perm in two launches: every batch of 256 pivots is composed into
+// its (dst <- src) list independently (one CTA per batch), then one CTA
+// applies the lists to iota in batch order.  work: per batch 1 + 2 * 512
+// ints (count, dst, src).
+constexpr int kPermBatch = 256;
+constexpr int kPermListInts = 1 + 4 * kPermBatch;
+
+__global__ void __launch_bounds__(1024) perm_compose_kernel(const int32_t* ipiv, int n, int32_t* work) {
+  __shared__ int p[kPermBatch], nxt[kPermBatch], lb[kPermBatch];
+  __shared__ int dst[2 * kPermBatch], src[2 * kPermBatch];
   __shared__ int s_m;
+  const int k0 = blockIdx.x * kPermBatch;
+  const int cnt = min(kPermBatch, n - k0);
+  const int m = compose_batch(ipiv, k0, cnt, p, nxt, lb, dst, src, &s_m);
+  int32_t* w = work + (int64_t)blockIdx.x * kPermListInts;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    w[1 + i] = dst[i];
+    w[1 + 2 * kPermBatch + i] = src[i];
+  }
+  if (threadIdx.x == 0) w[0] = m;
+}
+
+__global__ void __launch_bounds__(1024) perm_apply_lists_kernel(int n, int nb, const int32_t* work, int32_t* perm) {
+  __shared__ int vals[2 * kPermBatch];
   for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = i;
   __syncthreads();
-  for (int k0 = 0; k0 < n; k0 += 256) {
-    const int cnt = min(256, n - k0);
-    const int m = compose_batch(ipiv, k0, cnt, p, nxt, lb, dst, src, &s_m);
-    for (int i = threadIdx.x; i < m; i += blockDim.x) vals[i] = perm[src[i]];
+  for (int b = 0; b < nb; b++) {
+    const int32_t* w = work + (int64_t)b * kPermListInts;
+    const int m = w[0];
+    for (int i = threadIdx.x; i < m; i += blockDim.x) vals[i] = perm[w[1 + 2 * kPermBatch + i]];
     __syncthreads();
-    for (int i = threadIdx.x; i < m; i += blockDim.x) perm[dst[i]] = vals[i];
+    for (int i = threadIdx.x; i < m; i += blockDim.x) perm[w[1 + i]] = vals[i];
     __syncthreads();
   }
 }
@@ -158,9 +219,6 @@ __global__ void __launch_bounds__(1024) ipiv_apply_vector_kernel(const int32_t* 
   }
 }
 
-template <typename T>
-constexpr int apply_cs() { return 128 / (int)sizeof(T); }  // 128-byte row segments
-
 }  // namespace
 
 int launch_pivot_compose(const int32_t* ipiv, int k0, int cnt, const PivotList& pl, cudaStream_t s) {
@@ -174,26 +232,27 @@ int launch_pivot_compose(const int32_t* ipiv, int k0, int cnt, const PivotList& 
 template <typename T>
 int launch_pivot_apply(T* A, int64_t lda, int c_begin, int c_end, int skip_begin, int skip_end, const PivotList& pl,
                        int max_m, double* rhs, int32_t* perm, cudaStream_t s) {
-  constexpr int CS = apply_cs<T>();
+  constexpr int CS = 8 * (16 / (int)sizeof(T));
   if (c_end <= c_begin && !rhs && !perm) return LU_OK;
-  size_t smem = std::max((size_t)max_m * CS * sizeof(T), (size_t)max_m * (sizeof(double) + sizeof(int32_t)));
-  if (smem > 200 * 1024) return LU_ERR_ARG;
-  int strips = std::max(1, ceil_div(std::max(c_end - c_begin, 0), CS));
-  if (smem > 48 * 1024) {
-    static bool attr_set = false;
-    if (!attr_set) {
-      LUB_CUDA(cudaFuncSetAttribute(pivot_apply_kernel<T, CS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    200 * 1024));
-      attr_set = true;
-    }
-  }
-  pivot_apply_kernel<T, CS><<<strips, 256, smem, s>>>(A, lda, c_begin, c_end, skip_begin, skip_end, pl, rhs, perm);
+  if (max_m > 2 * kMaxBatch || max_m > kApplyThreads * kApplyUnroll / 8) return LU_ERR_ARG;
+  const int vec_ok = ((lda * (int64_t)sizeof(T)) % 16 == 0) && (reinterpret_cast<uintptr_t>(A) % 16 == 0) &&
+                     (c_begin % (16 / (int)sizeof(T)) == 0);
+  const int strips = std::max(1, ceil_div(std::max(c_end - c_begin, 0), CS));
+  pivot_apply_kernel<T><<<strips, kApplyThreads, 0, s>>>(A, lda, c_begin, c_end, skip_begin, skip_end, pl, rhs,
+                                                          perm, vec_ok);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }
 
+int ipiv_to_perm_work_ints(int n) { return ceil_div(std::max(n, 1), kPermBatch) * kPermListInts; }
+
 int launch_ipiv_to_perm(const int32_t* ipiv, int n, int32_t* perm, int32_t* work, cudaStream_t s) {
-  ipiv_to_perm_kernel<<<1, 1024, 0, s>>>(ipiv, n, perm, work);
+  if (n <= 0) return LU_OK;
+  if (!work) return LU_ERR_ARG;
+  const int nb = ceil_div(n, kPermBatch);
+  perm_compose_kernel<<<nb, 1024, 0, s>>>(ipiv, n, work);
+  LUB_LAUNCH_CHECK();
+  perm_apply_lists_kernel<<<1, 1024, 0, s>>>(n, nb, work, perm);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }

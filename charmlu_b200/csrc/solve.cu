@@ -388,10 +388,13 @@ __global__ void __launch_bounds__(256, 2) trsm_pipe_kernel(const TS* LU, int64_t
 }
 
 // G = -Lam * X^T (n x n), Lam and X n x k row-major, k <= 16: the rank-k
-// gradient of the adjoint.  Output-bound (8 n^2 bytes written).
+// gradient of the adjoint.  Output-bound (8 n^2 bytes written): each thread
+// keeps its two columns' X rows in registers and reads Lam rows as
+// warp-wide broadcasts, so shared-memory traffic stays well below the FMAs.
 __global__ void __launch_bounds__(256) neg_outer_kernel(const double* Lam, int64_t ldl, const double* X, int64_t ldx,
                                                         int n, int k, double* G, int64_t ldg, int accumulate) {
-  __shared__ double sl[64][17], sx[64][17];
+  __shared__ __align__(16) double sl[64][16];
+  __shared__ double sx[64][17];
   const int i0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
   for (int idx = threadIdx.x; idx < 64 * 16; idx += blockDim.x) {
     const int r = idx >> 4, c = idx & 15;
@@ -399,20 +402,33 @@ __global__ void __launch_bounds__(256) neg_outer_kernel(const double* Lam, int64
     sx[r][c] = (j0 + r < n && c < k) ? X[(int64_t)(j0 + r) * ldx + c] : 0.0;
   }
   __syncthreads();
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads, 2 x 8 outputs each
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads, 8 rows x 2 columns each
+  double xr0[16], xr1[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    xr0[q] = sx[tx][q];
+    xr1[q] = sx[tx + 32][q];
+  }
   for (int ri = 0; ri < 8; ri++) {
     const int r = ty * 8 + ri;
     if (i0 + r >= n) break;
+    double t0 = 0.0, t1 = 0.0;
 #pragma unroll
-    for (int cj = 0; cj < 2; cj++) {
-      const int c = tx + 32 * cj;
-      if (j0 + c >= n) continue;
-      double t = 0.0;
-#pragma unroll
-      for (int q = 0; q < 16; q++) t = fma(sl[r][q], sx[c][q], t);
-      double* g = &G[(int64_t)(i0 + r) * ldg + j0 + c];
-      if (accumulate) *g -= t;
-      else __stcs(g, -t);
+    for (int q = 0; q < 16; q += 2) {
+      const double2 l = *reinterpret_cast<const double2*>(&sl[r][q]);
+      t0 = fma(l.x, xr0[q], t0);
+      t1 = fma(l.x, xr1[q], t1);
+      t0 = fma(l.y, xr0[q + 1], t0);
+      t1 = fma(l.y, xr1[q + 1], t1);
+    }
+    double* g = &G[(int64_t)(i0 + r) * ldg + j0];
+    if (j0 + tx < n) {
+      if (accumulate) g[tx] -= t0;
+      else __stcs(&g[tx], -t0);
+    }
+    if (j0 + tx + 32 < n) {
+      if (accumulate) g[tx + 32] -= t1;
+      else __stcs(&g[tx + 32], -t1);
     }
   }
 }
