@@ -31,6 +31,14 @@ namespace lub {
 namespace {
 
 constexpr int THREADS = 256;
+// Columns are eliminated in groups of KG: a rank-1 update touches only the
+// rest of the current group, the columns past the group get one delayed
+// rank-KG update when the group ends, and a row that becomes a pivot row is
+// first brought up to date from the group's earlier pivot rows.  Every
+// element still sees the same FMAs in the same order as with immediate
+// rank-1 updates (bitwise the same factors), with about a third of the
+// shared-memory traffic.
+constexpr int KG = 8;
 
 template <typename T>
 __device__ __forceinline__ bool cand_better(T v1, int r1, T v2, int r2) {
@@ -79,6 +87,8 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
   __shared__ T s_v[9];
   __shared__ int s_r[9];
   __shared__ int s_p, s_win;
+  __shared__ T uhist[KG][W];     // pivot rows of the current group
+  __shared__ unsigned s_scaled;  // group columns whose pivot was usable
 
   const int G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x;
   const int r_lo = cta * R;
@@ -115,7 +125,8 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
       scr.cand_val[slot * kMaxLeafCTAs + cta] = cv;
       scr.cand_row[slot * kMaxLeafCTAs + cta] = cr;
     }
-    __threadfence();
+    // grid_barrier's CTA barrier followed by thread 0's release add makes
+    // these writes visible to every CTA that passes the barrier
     if (!grid_barrier(bar, (unsigned)(j + 1) * (unsigned)G, st, spin, 201)) return;
 
     // ---- global argmax over the G candidates
@@ -138,8 +149,22 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
                            : __ldcg(&scr.cand_data[((size_t)slot * kMaxLeafCTAs + s_win) * kMaxLeafW + tid]);
     }
     __syncthreads();
-    if (tid < ncols && p != j) {
-      if (p >= r_lo && p < r_hi) a[(p - r_lo) * LD + tid] = __ldcg(&scr.rowj[slot * kMaxLeafW + tid]);
+    // the pivot row's columns past the group still lack the group's earlier
+    // rank-1 updates (its multipliers are urow[g0 .. j))
+    const int g0 = (j / KG) * KG, g1 = min(ncols, g0 + KG);
+    if (j > g0) {
+      const unsigned mask = s_scaled;
+      if (tid >= g1 && tid < ncols) {
+        T v = urow[tid];
+        for (int t = g0; t < j; t++)
+          if ((mask >> (t - g0)) & 1u) v = fma(-urow[t], uhist[t - g0][tid], v);
+        urow[tid] = v;
+      }
+      __syncthreads();
+    }
+    if (tid < ncols) {
+      if (p != j && p >= r_lo && p < r_hi) a[(p - r_lo) * LD + tid] = __ldcg(&scr.rowj[slot * kMaxLeafW + tid]);
+      // position j takes the (brought up to date) pivot row, also when p == j
       if (j >= r_lo && j < r_hi) a[(j - r_lo) * LD + tid] = urow[tid];
     }
     // the swap on the enclosing panel's other columns (prow0: panel's first
@@ -163,25 +188,85 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
       ipiv[j] = row_base + p;
       if (!(fabs((double)piv) > thr)) dev_singular(st, info_base + j + 1);
     }
+    const bool do_scale = (piv != T(0)) && !isnan(piv);
+    if (tid < ncols) uhist[j - g0][tid] = urow[tid];
+    if (tid == 0) s_scaled = (j == g0 ? 0u : s_scaled) | (do_scale ? (1u << (j - g0)) : 0u);
     __syncthreads();
 
     // ---- multipliers, rank-1 update of the remaining leaf columns, and the
     //      candidate of column j+1 in the same pass
-    const bool do_scale = (piv != T(0)) && !isnan(piv);
     const bool has_next = j + 1 < ncols;
+    const bool delay = (j == g1 - 1) && (g1 < ncols);
+    const unsigned gmask = s_scaled;
     T bv = 0;
     int br = -1;
     const int r_first = max(j + 1 - r_lo, 0);
-    for (int r = r_first + tid; r < nr; r += THREADS) {
-      T* ar = a + r * LD;
+    // pivot-row values are warp-wide broadcasts.  A thread works on RU rows
+    // at once with explicit register staging (loads, then arithmetic, then
+    // stores), so the rows' shared-memory round trips and divisions overlap.
+    constexpr int RU = 4;
+    for (int rb = r_first + tid; rb < nr; rb += THREADS * RU) {
+      T* rp[RU];
+      bool live[RU];
+#pragma unroll
+      for (int u = 0; u < RU; u++) {
+        const int r = rb + u * THREADS;
+        live[u] = r < nr;
+        rp[u] = a + (size_t)(live[u] ? r : rb) * LD;
+      }
       if (do_scale) {
-        const T l = ar[j] / piv;
-        ar[j] = l;
-        for (int c = j + 1; c < ncols; c++) ar[c] = fma(-l, urow[c], ar[c]);
+        T l[RU];
+#pragma unroll
+        for (int u = 0; u < RU; u++) l[u] = live[u] ? rp[u][j] : T(0);
+#pragma unroll
+        for (int u = 0; u < RU; u++) l[u] = l[u] / piv;
+#pragma unroll
+        for (int u = 0; u < RU; u++)
+          if (live[u]) rp[u][j] = l[u];
+        for (int c = j + 1; c < g1; c++) {
+          const T uc = urow[c];
+          T v[RU];
+#pragma unroll
+          for (int u = 0; u < RU; u++) v[u] = live[u] ? rp[u][c] : T(0);
+#pragma unroll
+          for (int u = 0; u < RU; u++) v[u] = fma(-l[u], uc, v[u]);
+#pragma unroll
+          for (int u = 0; u < RU; u++)
+            if (live[u]) rp[u][c] = v[u];
+        }
+      }
+      if (delay) {  // the group's rank-KG update of the columns past it
+        T lv[RU][KG];
+#pragma unroll
+        for (int u = 0; u < RU; u++)
+#pragma unroll
+          for (int t = 0; t < KG; t++)
+            lv[u][t] = (live[u] && g0 + t < g1 && ((gmask >> t) & 1u)) ? rp[u][g0 + t] : T(0);
+        for (int c = g1; c < ncols; c++) {
+          T v[RU];
+#pragma unroll
+          for (int u = 0; u < RU; u++) v[u] = live[u] ? rp[u][c] : T(0);
+#pragma unroll
+          for (int t = 0; t < KG; t++) {
+            if (g0 + t < g1 && ((gmask >> t) & 1u)) {
+              const T uh = uhist[t][c];
+#pragma unroll
+              for (int u = 0; u < RU; u++) v[u] = fma(-lv[u][t], uh, v[u]);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < RU; u++)
+            if (live[u]) rp[u][c] = v[u];
+        }
       }
       if (has_next) {
-        T v = fabs(ar[j + 1]);
-        if (v > bv) { bv = v; br = r_lo + r; }
+#pragma unroll
+        for (int u = 0; u < RU; u++) {
+          if (live[u]) {
+            const T v = fabs(rp[u][j + 1]);
+            if (v > bv) { bv = v; br = r_lo + rb + u * THREADS; }
+          }
+        }
       }
     }
     block_argmax(bv, br, s_v, s_r, cv, cr);

@@ -176,6 +176,7 @@ __global__ void __launch_bounds__(256) trsv_kernel(const TS* LU, int64_t lda, in
       if (lane == 0) ok = wait_progress(&flags[0], q + 1, &v, st, spin, 301);
       ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
       seen = __shfl_sync(0xffffffffu, v, 0);
+      __syncwarp();  // lane 0's acquire orders the other lanes' reads of x
       if (!ok) break;
     }
     const int c = c0 + lane * 2;
@@ -212,7 +213,8 @@ __global__ void __launch_bounds__(256) trsv_kernel(const TS* LU, int64_t lda, in
     sum += __shfl_xor_sync(0xffffffffu, sum, 2);
     if (q4 == 0 && r < rows) x[r0 + r] = sum;
   }
-  __threadfence();
+  // CTA barrier, then thread 0's release store: the rows written above are
+  // visible to every CTA that acquires the counter
   __syncthreads();
   if (tid == 0) st_release_s32(&flags[0], tk + 1);
 }
@@ -382,7 +384,8 @@ __global__ void __launch_bounds__(256, 2) trsm_pipe_kernel(const TS* LU, int64_t
     const int r = m0 + g + (e >> 1) * 8, c = n0 + 2 * t + (e & 1);
     if (r < rows && c < nrhs) Y[(int64_t)(r0 + r) * ldy + c] = out[e];
   }
-  __threadfence();
+  // CTA barrier, then thread 0's release store: the rows written above are
+  // visible to every CTA that acquires the counter
   __syncthreads();
   if (tid == 0) st_release_s32(&flags[0], tk + 1);
 }
