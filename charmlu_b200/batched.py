@@ -89,3 +89,46 @@ def log_uniform_orders(count, lo=32, hi=1024, seed=42):
 def flops(n):
     n = np.asarray(n, dtype=np.float64)
     return float((2.0 / 3.0 * n ** 3 + 2.0 * n ** 2).sum())
+
+
+def partition_by_cost(n, parts):
+    """Split systems of orders n over `parts` GPUs so that the factor+solve
+    work (2/3 n^3 + 2 n^2 per system) is balanced: longest-processing-time
+    order, each system to the currently lightest part.  Deterministic;
+    returns `parts` sorted index arrays that together cover every system
+    exactly once.  The systems are independent, so a sharded run needs no
+    collective except the final gather_results."""
+    n = np.asarray(n, dtype=np.int64)
+    if parts < 1:
+        raise ValueError("parts must be >= 1")
+    cost = (2.0 / 3.0) * n.astype(np.float64) ** 3 + 2.0 * n.astype(np.float64) ** 2
+    order = np.argsort(-cost, kind="stable")
+    loads = np.zeros(parts)
+    buckets = [[] for _ in range(parts)]
+    for i in order:
+        p = int(np.argmin(loads))
+        buckets[p].append(int(i))
+        loads[p] += cost[i]
+    return [np.array(sorted(b), dtype=np.int64) for b in buckets]
+
+
+def gather_results(index, info, residual, count, group=None):
+    """Per-system status codes and scaled residuals of this rank's systems
+    (global indices `index`) gathered into global order on every rank over
+    torch.distributed (any backend).  Returns (info[count], residual[count])
+    as numpy arrays; systems no rank reported keep status -1 and NaN."""
+    import torch.distributed as dist
+    mine = (np.asarray(index, dtype=np.int64).tolist(), np.asarray(info, dtype=np.int64).tolist(),
+            np.asarray(residual, dtype=np.float64).tolist())
+    if dist.is_available() and dist.is_initialized():
+        allp = [None] * dist.get_world_size(group)
+        dist.all_gather_object(allp, mine, group=group)
+    else:
+        allp = [mine]
+    g_info = np.full(count, -1, dtype=np.int64)
+    g_res = np.full(count, np.nan)
+    for idx, inf, res in allp:
+        g_info[idx] = inf
+        g_res[idx] = res
+    return g_info, g_res
+
