@@ -559,3 +559,38 @@ template int launch_trsv<float>(const float*, int64_t, int, float*, int, int*, u
                                 cudaStream_t);
 
 }  // namespace lub
+
+namespace {
+// Test hook kernel: one thread waits on a progress counter that nothing
+// advances; the bounded wait must give up, record the timeout in the status
+// word and return.
+__global__ void wait_timeout_probe_kernel(const int* counter, lub::DevStatus* st, long long spin, int* out) {
+  int seen = 0;
+  const bool ok = lub::wait_progress(counter, 1, &seen, st, spin, 399);
+  *out = ok ? 1 : 0;
+}
+}  // namespace
+
+// Exercises the bounded pipeline wait on a counter that never advances
+// (failure detection without a fault): returns the status code the device
+// recorded (LU_ERR_TIMEOUT expected) or a CUDA error.
+extern "C" __attribute__((visibility("default"))) int lub_test_wait_timeout(long long spin) {
+  using namespace lub;
+  int* buf = nullptr;
+  if (cudaMalloc(&buf, 64) != cudaSuccess) return LU_ERR_NOMEM;
+  DevStatus* st = reinterpret_cast<DevStatus*>(buf + 4);
+  int* out = buf + 2;
+  cudaMemset(buf, 0, 64);
+  wait_timeout_probe_kernel<<<1, 1>>>(buf, st, spin, out);
+  int rc = cudaDeviceSynchronize() == cudaSuccess ? LU_OK : LU_ERR_CUDA;
+  DevStatus hst{};
+  int hout = -1;
+  if (rc == LU_OK) {
+    cudaMemcpy(&hst, st, sizeof(hst), cudaMemcpyDeviceToHost);
+    cudaMemcpy(&hout, out, sizeof(int), cudaMemcpyDeviceToHost);
+    rc = (hout == 0 && hst.code == LU_ERR_TIMEOUT) ? LU_ERR_TIMEOUT : (hst.code ? hst.code : LU_OK);
+  }
+  cudaFree(buf);
+  return rc;
+}
+
