@@ -37,25 +37,29 @@ __device__ __forceinline__ float scale_of(const unsigned* amax, int which) {
   return amax ? pow2_scale_of(__uint_as_float(amax[which])) : 1.f;
 }
 
-// dst[r][p*K + k] = part p of src[r][k] * scale (hi, or lo = rest after hi)
+// dst[r][p*ps + k] = part p of src[r][k] * scale (hi, or lo = rest after
+// hi); part p occupies [p*ps, p*ps + ps), zero past K (ps >= K)
 template <typename OUT>
 __global__ void split_rows_kernel(const float* __restrict__ src, int64_t lds, OUT* __restrict__ dst, int64_t ldd,
-                                  int rows, int K, int nparts, unsigned lo_mask, const unsigned* amax, int which) {
+                                  int rows, int K, int ps, int nparts, unsigned lo_mask, const unsigned* amax,
+                                  int which) {
   const int r = blockIdx.y * blockDim.y + threadIdx.y;
   if (r >= rows) return;
   const float sc = scale_of(amax, which);
-  for (int k = threadIdx.x; k < K; k += blockDim.x) {
-    const float v = src[(int64_t)r * lds + k] * sc;
+  for (int k = threadIdx.x; k < ps; k += blockDim.x) {
+    const float v = k < K ? src[(int64_t)r * lds + k] * sc : 0.f;
     const OUT hi = to_lp<OUT>(v);
     const OUT lo = to_lp<OUT>(v - from_lp(hi));
-    for (int p = 0; p < nparts; p++) dst[(int64_t)r * ldd + (int64_t)p * K + k] = ((lo_mask >> p) & 1) ? lo : hi;
+    for (int p = 0; p < nparts; p++) dst[(int64_t)r * ldd + (int64_t)p * ps + k] = ((lo_mask >> p) & 1) ? lo : hi;
   }
 }
 
-// dst[n][p*K + k] = part p of src[k][n] * scale: src is K x N, dst N x (nparts*K)
+// dst[n][p*ps + k] = part p of src[k][n] * scale: src is K x N, dst
+// N x (nparts*ps), zero past K in each part (ps >= K)
 template <typename OUT>
 __global__ void split_transpose_kernel(const float* __restrict__ src, int64_t lds, OUT* __restrict__ dst, int64_t ldd,
-                                       int K, int N, int nparts, unsigned lo_mask, const unsigned* amax, int which) {
+                                       int K, int ps, int N, int nparts, unsigned lo_mask, const unsigned* amax,
+                                       int which) {
   __shared__ float t[32][33];
   const int k0 = blockIdx.y * 32, n0 = blockIdx.x * 32;
   const float sc = scale_of(amax, which);
@@ -66,11 +70,11 @@ __global__ void split_transpose_kernel(const float* __restrict__ src, int64_t ld
   __syncthreads();
   for (int i = threadIdx.y; i < 32; i += blockDim.y) {
     const int n = n0 + i, k = k0 + threadIdx.x;
-    if (n < N && k < K) {
-      const float v = t[threadIdx.x][i];
+    if (n < N && k < ps) {
+      const float v = t[threadIdx.x][i];  // zero past K (staged above)
       const OUT hi = to_lp<OUT>(v);
       const OUT lo = to_lp<OUT>(v - from_lp(hi));
-      for (int p = 0; p < nparts; p++) dst[(int64_t)n * ldd + (int64_t)p * K + k] = ((lo_mask >> p) & 1) ? lo : hi;
+      for (int p = 0; p < nparts; p++) dst[(int64_t)n * ldd + (int64_t)p * ps + k] = ((lo_mask >> p) & 1) ? lo : hi;
     }
   }
 }
@@ -213,32 +217,36 @@ int launch_f64_to_f32(const double* src, int64_t lds, float* dst, int64_t ldd, i
 
 template <typename OUT>
 int launch_split_rows(const float* src, int64_t lds, OUT* dst, int64_t ldd, int rows, int K, int nparts,
-                      unsigned lo_mask, const unsigned* amax, int which, cudaStream_t s) {
+                      unsigned lo_mask, const unsigned* amax, int which, cudaStream_t s, int part_stride) {
   if (rows <= 0 || K <= 0) return LU_OK;
+  const int ps = part_stride > 0 ? part_stride : K;
+  if (ps < K) return LU_ERR_ARG;
   dim3 block(128, 4);
   dim3 grid(1, ceil_div(rows, 4));
-  split_rows_kernel<OUT><<<grid, block, 0, s>>>(src, lds, dst, ldd, rows, K, nparts, lo_mask, amax, which);
+  split_rows_kernel<OUT><<<grid, block, 0, s>>>(src, lds, dst, ldd, rows, K, ps, nparts, lo_mask, amax, which);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }
 template <typename OUT>
 int launch_split_transpose(const float* src, int64_t lds, OUT* dst, int64_t ldd, int K, int N, int nparts,
-                           unsigned lo_mask, const unsigned* amax, int which, cudaStream_t s) {
+                           unsigned lo_mask, const unsigned* amax, int which, cudaStream_t s, int part_stride) {
   if (K <= 0 || N <= 0) return LU_OK;
+  const int ps = part_stride > 0 ? part_stride : K;
+  if (ps < K) return LU_ERR_ARG;
   dim3 block(32, 8);
-  dim3 grid(ceil_div(N, 32), ceil_div(K, 32));
-  split_transpose_kernel<OUT><<<grid, block, 0, s>>>(src, lds, dst, ldd, K, N, nparts, lo_mask, amax, which);
+  dim3 grid(ceil_div(N, 32), ceil_div(ps, 32));
+  split_transpose_kernel<OUT><<<grid, block, 0, s>>>(src, lds, dst, ldd, K, ps, N, nparts, lo_mask, amax, which);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }
 template int launch_split_rows<__nv_bfloat16>(const float*, int64_t, __nv_bfloat16*, int64_t, int, int, int, unsigned,
-                                              const unsigned*, int, cudaStream_t);
+                                              const unsigned*, int, cudaStream_t, int);
 template int launch_split_rows<__half>(const float*, int64_t, __half*, int64_t, int, int, int, unsigned,
-                                       const unsigned*, int, cudaStream_t);
+                                       const unsigned*, int, cudaStream_t, int);
 template int launch_split_transpose<__nv_bfloat16>(const float*, int64_t, __nv_bfloat16*, int64_t, int, int, int,
-                                                   unsigned, const unsigned*, int, cudaStream_t);
+                                                   unsigned, const unsigned*, int, cudaStream_t, int);
 template int launch_split_transpose<__half>(const float*, int64_t, __half*, int64_t, int, int, int, unsigned,
-                                            const unsigned*, int, cudaStream_t);
+                                            const unsigned*, int, cudaStream_t, int);
 
 int launch_panel_absmax(const float* L, int64_t ldl, int rows, int K, const float* U, int64_t ldu, int N,
                         unsigned* amax, cudaStream_t s) {

@@ -101,6 +101,7 @@ struct Bf16GemmArgs {
   const unsigned* amax;  // per-panel |L|max, |U|max bit patterns (scaled FP16 operands) or null
   DevStatus* st;
   long long spin;
+  int kpart;    // pairs layout: element offset of the lo parts (K = kpart); 0 otherwise
 };
 
 __global__ void __launch_bounds__(THREADS, 1)
@@ -227,19 +228,31 @@ gemm_bf16_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_const
 // ---------------------------------------------------------------------------
 constexpr int P_THREADS = 192;
 constexpr int P_TMEM_COLS = 512;
+// Pairs layout (error-compensated FP16): one stage holds the hi and lo parts
+// of an L and a U k-block (Lh, Ll, Uh, Ul) and feeds three MMAs per 16-wide
+// k step (Lh*Uh, Lh*Ul, Ll*Uh), so each part is loaded once instead of the
+// three [hi,hi,lo] x [hi,lo,hi] k-blocks of the plain layout (a third less
+// operand traffic per MMA).  Two stages fit beside the epilogue boxes.
+constexpr int PAIR_STAGES = 2;
+constexpr int PAIR_STAGE_BYTES = 2 * STAGE_BYTES;  // 96 KB
+constexpr int PAIR_SMEM_BYTES = PAIR_STAGES * PAIR_STAGE_BYTES + 2 * EPI_BYTES + 1024 + 256;
+static_assert(PAIR_SMEM_BYTES <= 227 * 1024, "pairs layout exceeds shared memory");
 
 __device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
+template <bool PAIRS>
 __global__ void __launch_bounds__(P_THREADS, 1)
 gemm_lowp_persistent_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                             const __grid_constant__ CUtensorMap mapC, Bf16GemmArgs args) {
+  constexpr int NST = PAIRS ? PAIR_STAGES : STAGES;
+  constexpr int SB = PAIRS ? PAIR_STAGE_BYTES : STAGE_BYTES;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  unsigned char* epi = smem + STAGES * STAGE_BYTES;
+  unsigned char* epi = smem + NST * SB;
   uint64_t* full = reinterpret_cast<uint64_t*>(epi + 2 * EPI_BYTES);
-  uint64_t* empty = full + STAGES;
-  uint64_t* tfull = empty + STAGES;
+  uint64_t* empty = full + NST;
+  uint64_t* tfull = empty + NST;
   uint64_t* tempty = tfull + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
   __shared__ int s_epi_fail;  // sticky: the epilogue warps stop together
@@ -254,7 +267,7 @@ gemm_lowp_persistent_kernel(const __grid_constant__ CUtensorMap mapA, const __gr
     prefetch_tmap(&mapA);
     prefetch_tmap(&mapB);
     prefetch_tmap(&mapC);
-    for (int s = 0; s < STAGES; s++) {
+    for (int s = 0; s < NST; s++) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
@@ -284,15 +297,22 @@ gemm_lowp_persistent_kernel(const __grid_constant__ CUtensorMap mapA, const __gr
         int tm, tn;
         grouped_tile(t, ntm, ntn, 16, tm, tn);
         for (int kt = 0; kt < KT; kt++, kb++) {
-          const int s = (int)(kb % STAGES);
-          if (kb >= STAGES && !mbar_wait(&empty[s], (uint32_t)(((kb / STAGES) - 1) & 1), args.st, lim, 411)) {
+          const int s = (int)(kb % NST);
+          if (kb >= NST && !mbar_wait(&empty[s], (uint32_t)(((kb / NST) - 1) & 1), args.st, lim, 411)) {
             ok = false;
             break;
           }
-          unsigned char* sa = smem + s * STAGE_BYTES;
-          mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
-          tma_load_2d(sa, &mapA, &full[s], kt * BK, args.a_row0 + tm * BM);
-          tma_load_2d(sa + A_BYTES, &mapB, &full[s], kt * BK, args.b_row0 + tn * BN);
+          unsigned char* sa = smem + s * SB;
+          mbar_arrive_expect_tx(&full[s], SB);
+          if (PAIRS) {  // [Lh | Ll | Uh | Ul]
+            tma_load_2d(sa, &mapA, &full[s], kt * BK, args.a_row0 + tm * BM);
+            tma_load_2d(sa + A_BYTES, &mapA, &full[s], args.kpart + kt * BK, args.a_row0 + tm * BM);
+            tma_load_2d(sa + 2 * A_BYTES, &mapB, &full[s], kt * BK, args.b_row0 + tn * BN);
+            tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &mapB, &full[s], args.kpart + kt * BK, args.b_row0 + tn * BN);
+          } else {
+            tma_load_2d(sa, &mapA, &full[s], kt * BK, args.a_row0 + tm * BM);
+            tma_load_2d(sa + A_BYTES, &mapB, &full[s], kt * BK, args.b_row0 + tn * BN);
+          }
         }
       }
     }
@@ -307,18 +327,32 @@ gemm_lowp_persistent_kernel(const __grid_constant__ CUtensorMap mapA, const __gr
         tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(ab * 256);
         for (int kt = 0; kt < KT; kt++, kb++) {
-          const int s = (int)(kb % STAGES);
-          if (!mbar_wait(&full[s], (uint32_t)((kb / STAGES) & 1), args.st, lim, 413)) {
+          const int s = (int)(kb % NST);
+          if (!mbar_wait(&full[s], (uint32_t)((kb / NST) & 1), args.st, lim, 413)) {
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint32_t a_addr = smem_u32(smem + s * STAGE_BYTES);
-          const uint32_t b_addr = a_addr + A_BYTES;
+          const uint32_t a_addr = smem_u32(smem + s * SB);
+          if (PAIRS) {
+            const uint32_t al_addr = a_addr + A_BYTES;
+            const uint32_t bh_addr = a_addr + 2 * A_BYTES;
+            const uint32_t bl_addr = bh_addr + B_BYTES;
 #pragma unroll
-          for (int kk = 0; kk < BK / 16; kk++)
-            umma_f16(d, smem_desc_k128(a_addr + kk * 32), smem_desc_k128(b_addr + kk * 32), args.idesc,
-                     (kt > 0 || kk > 0) ? 1u : 0u);
+            for (int kk = 0; kk < BK / 16; kk++) {
+              const uint64_t ah = smem_desc_k128(a_addr + kk * 32), al = smem_desc_k128(al_addr + kk * 32);
+              const uint64_t bh = smem_desc_k128(bh_addr + kk * 32), bl = smem_desc_k128(bl_addr + kk * 32);
+              umma_f16(d, ah, bh, args.idesc, (kt > 0 || kk > 0) ? 1u : 0u);
+              umma_f16(d, ah, bl, args.idesc, 1u);
+              umma_f16(d, al, bh, args.idesc, 1u);
+            }
+          } else {
+            const uint32_t b_addr = a_addr + A_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; kk++)
+              umma_f16(d, smem_desc_k128(a_addr + kk * 32), smem_desc_k128(b_addr + kk * 32), args.idesc,
+                       (kt > 0 || kk > 0) ? 1u : 0u);
+          }
           umma_commit(&empty[s]);
         }
         umma_commit(&tfull[ab]);
@@ -384,21 +418,30 @@ gemm_lowp_persistent_kernel(const __grid_constant__ CUtensorMap mapA, const __gr
 
 int gemm_bf16_init() {
   LUB_CUDA(cudaFuncSetAttribute(gemm_bf16_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-  LUB_CUDA(
-      cudaFuncSetAttribute(gemm_lowp_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+  LUB_CUDA(cudaFuncSetAttribute(gemm_lowp_persistent_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                SMEM_BYTES));
+  LUB_CUDA(cudaFuncSetAttribute(gemm_lowp_persistent_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                PAIR_SMEM_BYTES));
   return LU_OK;
 }
 
-// Persistent launch: grid = min(tiles, max_ctas).
+// Persistent launch: grid = min(tiles, max_ctas).  kpart > 0 selects the
+// pairs layout: operand rows [hi (kpart) | lo (kpart)], K = kpart, a
+// multiple of the 64-wide k block.
 int launch_gemm_lowp_persistent(const CUtensorMap& mapA, const CUtensorMap& mapB, const CUtensorMap& mapC,
                                 int a_row0, int b_row0, int c_row0, int c_col0, int M, int N, int K, bool bf16,
-                                const unsigned* amax, DevStatus* st, long long spin, int max_ctas, cudaStream_t s) {
+                                const unsigned* amax, DevStatus* st, long long spin, int max_ctas, cudaStream_t s,
+                                int kpart) {
   if (M <= 0 || N <= 0 || K <= 0) return LU_OK;
   if (c_col0 & 3) return LU_ERR_ALIGN;
-  Bf16GemmArgs a{a_row0, b_row0, c_row0, c_col0, M, N, K, make_idesc(bf16), amax, st, spin};
+  if (kpart > 0 && (kpart != K || (kpart % BK) || bf16)) return LU_ERR_ARG;
+  Bf16GemmArgs a{a_row0, b_row0, c_row0, c_col0, M, N, K, make_idesc(bf16), amax, st, spin, kpart};
   const int64_t tiles = (int64_t)ceil_div(N, BN) * ceil_div(M, BM);
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, std::max(1, max_ctas)));
-  gemm_lowp_persistent_kernel<<<grid, P_THREADS, SMEM_BYTES, s>>>(mapA, mapB, mapC, a);
+  if (kpart > 0)
+    gemm_lowp_persistent_kernel<true><<<grid, P_THREADS, PAIR_SMEM_BYTES, s>>>(mapA, mapB, mapC, a);
+  else
+    gemm_lowp_persistent_kernel<false><<<grid, P_THREADS, SMEM_BYTES, s>>>(mapA, mapB, mapC, a);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }
@@ -434,15 +477,20 @@ extern "C" __attribute__((visibility("default"))) int lub_test_gemm_lowp(const f
                                                                          int N, int K, int mode, void* stream) {
   using namespace lub;
   cudaStream_t s = (cudaStream_t)stream;
-  // mode bits 0-7: 0 bf16, 1 scaled fp16, 2 split fp16 x3; bits 8+: CTA count
-  // of the persistent kernel (0: one CTA per tile)
+  // mode bits 0-7: 0 bf16, 1 scaled fp16, 2 split fp16 x3 (concatenated
+  // parts), 3 split fp16 x3 in the pairs layout (persistent kernel only);
+  // bits 8+: CTA count of the persistent kernel (0: one CTA per tile)
   const int pctas = mode >> 8;
   mode &= 0xff;
-  if (M <= 0 || N <= 0 || K <= 0 || mode < 0 || mode > 2 || (ldc & 3) || (reinterpret_cast<uintptr_t>(C) & 15))
+  if (M <= 0 || N <= 0 || K <= 0 || mode < 0 || mode > 3 || (ldc & 3) || (reinterpret_cast<uintptr_t>(C) & 15))
     return LU_ERR_ARG;
+  if (mode == 3 && pctas <= 0) return LU_ERR_ARG;
   LUB_TRY(gemm_bf16_init());
-  const int nparts = mode == 2 ? 3 : 1;
-  const int Ke = nparts * K;
+  const bool pairs = mode == 3;
+  const int nparts = mode == 2 ? 3 : (pairs ? 2 : 1);
+  const int kps = (K + 63) & ~63;
+  const int Ke = pairs ? 2 * kps : nparts * K;  // tensor-map width
+  const int Kg = pairs ? kps : Ke;               // GEMM k extent
   const int64_t ldk = (Ke + 63) & ~int64_t(63);
   __nv_bfloat16 *Lb = nullptr, *Ub = nullptr;
   LUB_CUDA(cudaMalloc(&Lb, sizeof(__nv_bfloat16) * M * ldk));
@@ -458,11 +506,13 @@ extern "C" __attribute__((visibility("default"))) int lub_test_gemm_lowp(const f
     if (rc == LU_OK) rc = launch_split_transpose<__nv_bfloat16>(B, ldb, Ub, ldk, K, N, 1, 0u, nullptr, 1, s);
   } else {
     rc = launch_panel_absmax(A, lda, M, K, B, ldb, N, amax, s);
+    const unsigned lmask = pairs ? 0x2u : 0x4u;
     if (rc == LU_OK)
-      rc = launch_split_rows<__half>(A, lda, reinterpret_cast<__half*>(Lb), ldk, M, K, nparts, 0x4u, amax, 0, s);
+      rc = launch_split_rows<__half>(A, lda, reinterpret_cast<__half*>(Lb), ldk, M, K, nparts, lmask, amax, 0, s,
+                                     pairs ? kps : 0);
     if (rc == LU_OK)
       rc = launch_split_transpose<__half>(B, ldb, reinterpret_cast<__half*>(Ub), ldk, K, N, nparts, 0x2u, amax, 1,
-                                          s);
+                                          s, pairs ? kps : 0);
   }
   const CUtensorMapDataType dt = bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
   CUtensorMap mL, mU, mC;
@@ -471,8 +521,8 @@ extern "C" __attribute__((visibility("default"))) int lub_test_gemm_lowp(const f
   if (rc == LU_OK)
     rc = encode_tmap_2d(&mC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, N, M, ldc * 4, 32, 128, CU_TENSOR_MAP_SWIZZLE_128B);
   if (rc == LU_OK && pctas > 0)
-    rc = launch_gemm_lowp_persistent(mL, mU, mC, 0, 0, 0, 0, M, N, Ke, bf16, bf16 ? nullptr : amax, st, 1LL << 24,
-                                     pctas, s);
+    rc = launch_gemm_lowp_persistent(mL, mU, mC, 0, 0, 0, 0, M, N, Kg, bf16, bf16 ? nullptr : amax, st, 1LL << 24,
+                                     pctas, s, pairs ? kps : 0);
   else if (rc == LU_OK)
     rc = launch_gemm_bf16_tc(mL, mU, mC, 0, 0, 0, 0, M, N, Ke, bf16, bf16 ? nullptr : amax, st, 1LL << 24, s);
   DevStatus hst{};

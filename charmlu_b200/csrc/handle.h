@@ -74,7 +74,8 @@ struct lu_handle_s {
   int64_t ldk = 0;
   int32_t* ipiv32 = nullptr;   // pivots of the low-precision factorisation
   unsigned* amax = nullptr;    // per-panel |L|max, |U|max (scaled FP16 operands)
-  int nparts = 1;              // 3 for the error-compensated FP16 split
+  int nparts = 1;              // 3 for the error-compensated FP16 split (2 in the pairs layout)
+  bool pairs = false;          // FP16x3 operands as [hi | lo] for the persistent update
   float* v32 = nullptr;        // FP32 work vector (solves)
   double* r64 = nullptr;       // FP64 residual
   double* z64 = nullptr;       // FP64 work vector (GMRES)

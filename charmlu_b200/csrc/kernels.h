@@ -129,22 +129,27 @@ int gemm_bf16_init();
 int launch_gemm_bf16_tc(const CUtensorMap& mapA, const CUtensorMap& mapB, const CUtensorMap& mapC, int a_row0,
                         int b_row0, int c_row0, int c_col0, int M, int N, int K, bool bf16, const unsigned* amax,
                         DevStatus* st, long long spin, cudaStream_t s);
-// persistent variant: max_ctas CTAs walk the tiles (TMEM double-buffered)
+// persistent variant: max_ctas CTAs walk the tiles (TMEM double-buffered);
+// kpart > 0: error-compensated pairs layout [hi | lo] per operand row, the
+// three products Lh*Uh + Lh*Ul + Ll*Uh from one stage, K = kpart
 int launch_gemm_lowp_persistent(const CUtensorMap& mapA, const CUtensorMap& mapB, const CUtensorMap& mapC,
                                 int a_row0, int b_row0, int c_row0, int c_col0, int M, int N, int K, bool bf16,
-                                const unsigned* amax, DevStatus* st, long long spin, int max_ctas, cudaStream_t s);
+                                const unsigned* amax, DevStatus* st, long long spin, int max_ctas, cudaStream_t s,
+                                int kpart = 0);
 // |max| of the L21 (rows x K) and U12 (K x N) FP32 panels into amax[0], amax[1]
 int launch_panel_absmax(const float* L, int64_t ldl, int rows, int K, const float* U, int64_t ldu, int N,
                         unsigned* amax, cudaStream_t s);
 // low-precision operand panels: nparts K-wide copies, part p is the hi
 // (bit p of lo_mask clear) or lo (set) component of src * scale, scale the
 // power of two of amax[which] (or 1 when amax is null); OUT bf16 or fp16
+// (part_stride > 0: part p starts at p * part_stride, zero-filled past K;
+// 0: parts are K wide and contiguous)
 template <typename OUT>
 int launch_split_rows(const float* src, int64_t lds, OUT* dst, int64_t ldd, int rows, int K, int nparts,
-                      unsigned lo_mask, const unsigned* amax, int which, cudaStream_t s);
+                      unsigned lo_mask, const unsigned* amax, int which, cudaStream_t s, int part_stride = 0);
 template <typename OUT>
 int launch_split_transpose(const float* src, int64_t lds, OUT* dst, int64_t ldd, int K, int N, int nparts,
-                           unsigned lo_mask, const unsigned* amax, int which, cudaStream_t s);
+                           unsigned lo_mask, const unsigned* amax, int which, cudaStream_t s, int part_stride = 0);
 int launch_f64_to_f32(const double* src, int64_t lds, float* dst, int64_t ldd, int rows, int cols, cudaStream_t s);
 int launch_ir_prep(const double* r64, const int32_t* perm, float* r32, int n, const ResidualAccum* acc,
                    cudaStream_t s);

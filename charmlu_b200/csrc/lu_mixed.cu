@@ -29,8 +29,11 @@ int ensure_mixed(lu_handle h) {
   const int64_t n = h->cfg.n;
   const int64_t B = h->cfg.block_size;
   h->ld32 = (n + 31) & ~int64_t(31);
-  h->nparts = h->cfg.precision == LU_PREC_FP16X3 ? 3 : 1;
-  h->ldk = (h->nparts * B + 63) & ~int64_t(63);
+  // FP16x3 on the persistent update: operand rows [hi | lo], each part a
+  // whole number of 64-wide k blocks; otherwise the parts are concatenated
+  h->pairs = h->cfg.precision == LU_PREC_FP16X3 && h->gemm_ctas > 0;
+  h->nparts = h->cfg.precision == LU_PREC_FP16X3 ? (h->pairs ? 2 : 3) : 1;
+  h->ldk = h->pairs ? 2 * ((B + 63) & ~int64_t(63)) : (h->nparts * B + 63) & ~int64_t(63);
   h->gm = kGmresRestart;
   LUB_TRY(h->alloc(&h->A32, (size_t)n * h->ld32));
   LUB_TRY(h->alloc(&h->Lb, (size_t)n * h->ldk));
@@ -115,17 +118,29 @@ int panel32(Ctx32& c, int c0, int w, int p0, int pw) {
 }
 
 // Low-precision operand panels of step k (L21 rows k1.., U12^T) and their
-// tensor maps; K' = nparts * kw.
+// tensor maps.  *K is the GEMM's k extent and *kpart the pairs layout's lo
+// offset (0 when the parts are concatenated: K = nparts * kw).
 int build_operands(lu_handle h, const Ctx32& c, int k0, int kw, int k1, int rest, bool bf16, CUtensorMap* mapL,
-                   CUtensorMap* mapU, cudaStream_t s) {
+                   CUtensorMap* mapU, int* K, int* kpart, cudaStream_t s) {
   const float* L21 = c.A + (int64_t)k1 * c.ld + k0;
   const float* U12 = c.A + (int64_t)k0 * c.ld + k1;
-  const int ke = h->nparts * kw;
+  const bool pairs = !bf16 && h->pairs;
+  const int kps = (kw + 63) & ~63;
+  const int ke = pairs ? 2 * kps : h->nparts * kw;  // tensor-map width
+  *K = pairs ? kps : ke;
+  *kpart = pairs ? kps : 0;
   {
     Prof pf(h, s, LU_PH_OTHER);
     if (bf16) {
       LUB_TRY(launch_split_rows<__nv_bfloat16>(L21, c.ld, h->Lb, h->ldk, rest, kw, 1, 0u, nullptr, 0, s));
       LUB_TRY(launch_split_transpose<__nv_bfloat16>(U12, c.ld, h->Ub, h->ldk, kw, rest, 1, 0u, nullptr, 1, s));
+    } else if (pairs) {
+      // [Lh | Ll] and [Uh | Ul], each part kps wide (zero past kw)
+      LUB_TRY(launch_panel_absmax(L21, c.ld, rest, kw, U12, c.ld, rest, h->amax, s));
+      LUB_TRY(launch_split_rows<__half>(L21, c.ld, reinterpret_cast<__half*>(h->Lb), h->ldk, rest, kw, 2, 0x2u,
+                                        h->amax, 0, s, kps));
+      LUB_TRY(launch_split_transpose<__half>(U12, c.ld, reinterpret_cast<__half*>(h->Ub), h->ldk, kw, rest, 2, 0x2u,
+                                             h->amax, 1, s, kps));
     } else {
       // L parts [hi, hi, lo] against U parts [hi, lo, hi]: Lh*Uh + Lh*Ul + Ll*Uh
       LUB_TRY(launch_panel_absmax(L21, c.ld, rest, kw, U12, c.ld, rest, h->amax, s));
@@ -142,15 +157,18 @@ int build_operands(lu_handle h, const Ctx32& c, int k0, int kw, int k1, int rest
 }
 
 // C(k1.., c0..c0+ncols) -= L21 * U12[:, u0..u0+ncols] on the tensor cores
-// (reserve: SMs left free for a panel running beside it)
+// (reserve: SMs left free for a panel running beside it).  K and kpart as
+// from build_operands; flops are counted as executed on the panel's kw
+// columns (three products for the FP16 split).
 int lowp_gemm(lu_handle h, const CUtensorMap& mapL, const CUtensorMap& mapU, const CUtensorMap& mapC, int k1,
-              int rest, int u0, int ncols, int ke, bool bf16, cudaStream_t s, int reserve = 0) {
-  Prof pf(h, s, LU_PH_GEMM, 2.0 * rest * (double)ncols * ke);
+              int rest, int u0, int ncols, int K, int kpart, int kw, bool bf16, cudaStream_t s, int reserve = 0) {
+  const int prods = bf16 ? 1 : (h->cfg.precision == LU_PREC_FP16X3 ? 3 : 1);
+  Prof pf(h, s, LU_PH_GEMM, 2.0 * rest * (double)ncols * kw * prods);
   const unsigned* amax = bf16 ? nullptr : h->amax;
   if (h->gemm_ctas > 0)
-    return launch_gemm_lowp_persistent(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, ke, bf16, amax, h->st,
-                                       h->spin, std::max(1, h->gemm_ctas - reserve), s);
-  return launch_gemm_bf16_tc(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, ke, bf16, amax, h->st, h->spin, s);
+    return launch_gemm_lowp_persistent(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, K, bf16, amax, h->st,
+                                       h->spin, std::max(1, h->gemm_ctas - reserve), s, kpart);
+  return launch_gemm_bf16_tc(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, K, bf16, amax, h->st, h->spin, s);
 }
 
 // LU of h->A32 in place: FP32 panels/TRSM, low-precision tcgen05 trailing
@@ -176,8 +194,9 @@ int factor_mixed(lu_handle h, cudaStream_t s) {
       if (rest <= 0) continue;
       LUB_TRY(trsm32(c, k0, kw, k0, k1, rest));
       CUtensorMap mapL, mapU;
-      LUB_TRY(build_operands(h, c, k0, kw, k1, rest, bf16, &mapL, &mapU, s));
-      LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, 0, rest, h->nparts * kw, bf16, s));
+      int K = 0, kpart = 0;
+      LUB_TRY(build_operands(h, c, k0, kw, k1, rest, bf16, &mapL, &mapU, &K, &kpart, s));
+      LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, 0, rest, K, kpart, kw, bf16, s));
     }
     return LU_OK;
   }
@@ -195,14 +214,16 @@ int factor_mixed(lu_handle h, cudaStream_t s) {
     if (rest <= 0) continue;
     LUB_TRY(trsm32(c, k0, kw, k0, k1, rest));
     CUtensorMap mapL, mapU;
-    LUB_TRY(build_operands(h, c, k0, kw, k1, rest, bf16, &mapL, &mapU, s));
-    const int nw = std::min(B, rest), ke = h->nparts * kw;
-    LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, 0, nw, ke, bf16, s));  // next panel's columns
+    int K = 0, kpart = 0;
+    LUB_TRY(build_operands(h, c, k0, kw, k1, rest, bf16, &mapL, &mapU, &K, &kpart, s));
+    const int nw = std::min(B, rest);
+    LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, 0, nw, K, kpart, kw, bf16, s));  // next panel's columns
     LUB_CUDA(cudaEventRecord(h->evN, s));
     LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evN, 0));
     LUB_TRY(panel32(cp, k1, nw, k1, nw));
     LUB_CUDA(cudaEventRecord(h->evP, h->sP));
-    if (rest > nw) LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, nw, rest - nw, ke, bf16, s, h->gemm_reserve));
+    if (rest > nw)
+      LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, nw, rest - nw, K, kpart, kw, bf16, s, h->gemm_reserve));
   }
   return LU_OK;
 }

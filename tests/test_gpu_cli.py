@@ -1,0 +1,48 @@
+"""The CLI as a drop-in for test_lu.pl (test_lu.pl:9-84): every parameter
+set of its five tables (block sizes, pivot agglomeration batch sizes,
+mapping arguments, medium and large sizes) through
+`python -m charmlu_b200 N b mem [batch mapping ...]`, graded the way
+test_lu.pl grades it: the `residual = X` line must give X < 16."""
+import os
+import re
+import subprocess
+import sys
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+# test_lu.pl's tables: smalltests, agglomtests, mappingtests, mediumtests, largetests
+TEST_LU_PL_ARGS = [
+    [48, 48, 500], [48, 24, 500], [48, 16, 500], [48, 12, 500],
+    [32, 8, 500, 9], [32, 8, 500, 8], [32, 8, 500, 7], [32, 8, 500, 4], [32, 8, 500, 3], [32, 8, 500, 2],
+    [32, 8, 500, 1], [32, 4, 500, 2], [32, 4, 500, 1],
+    [512, 128, 500, 128, 2], [512, 128, 500, 128, 3], [512, 64, 500, 128, 3, 4, 1],
+    [512, 64, 500, 128, 3, 4, 1, 1], [512, 64, 500, 128, 3, 4, 1, 2], [512, 64, 500, 128, 3, 1, 4, 2, 4],
+    [512, 64, 500, 128, 3, 1, 4, 2, 2], [512, 64, 500, 128, 3, 1, 4, 2, 1],
+    [512, 256, 500], [512, 128, 500], [1024, 256, 500], [1024, 128, 500], [1024, 64, 500],
+    [2048, 256, 500], [2048, 512, 500], [4096, 256, 500], [4096, 512, 500],
+]
+RESIDUAL = re.compile(r"residual = ([\d\.]*)")  # test_lu.pl:77
+
+
+@pytest.mark.parametrize("args", TEST_LU_PL_ARGS, ids=lambda a: "_".join(map(str, a)))
+def test_cli_residual_line(cuda_dev, capsys, args):
+    from charmlu_b200.__main__ import main
+    assert main([str(v) for v in args]) in (0, None)
+    out = capsys.readouterr().out
+    m = RESIDUAL.search(out)
+    assert m is not None, out
+    assert float(m.group(1)) < 16, out
+    assert "RESULT procs:" in out and "HPL flop count gives" in out
+    assert f"Pivot batch size: {args[3] if len(args) > 3 else args[1] // 4}" in out
+
+
+def test_cli_process_entry_point(cuda_dev):
+    r = subprocess.run([sys.executable, "-m", "charmlu_b200", "48", "12", "500"], cwd=ROOT, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    m = RESIDUAL.search(r.stdout)
+    assert m is not None and float(m.group(1)) < 16, r.stdout

@@ -33,7 +33,9 @@ def _pow2_scale(t):
 def _lowp_reference(A, B, C, mode):
     """C - product, the product formed exactly (FP64) from the operands the
     kernel sees: BF16-rounded (mode 0), FP16 of the power-of-two scaled
-    panel (mode 1), or the hi/lo FP16 split with three products (mode 2)."""
+    panel (mode 1), or the hi/lo FP16 split with three products (mode 2;
+    mode 3, the pairs layout, computes the same three products)."""
+    mode = 2 if mode == 3 else mode
     if mode == 0:
         return C.double() - A.bfloat16().double() @ B.bfloat16().double()
     sa, sb = _pow2_scale(A), _pow2_scale(B)
@@ -48,9 +50,9 @@ def _lowp_reference(A, B, C, mode):
     return C.double() - P / (sa * sb)
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
 @pytest.mark.parametrize("M,N,K", [(128, 256, 64), (300, 520, 256), (1024, 1024, 512), (257, 999, 1024),
-                                   (4096, 4096, 256)])
+                                   (4096, 4096, 256), (1000, 700, 200)])
 def test_gemm_lowp_tcgen05_matches_reference(cuda_dev, M, N, K, mode):
     f = _lib()
     g = torch.Generator(device="cuda").manual_seed(M * 7 + N)
@@ -61,17 +63,18 @@ def test_gemm_lowp_tcgen05_matches_reference(cuda_dev, M, N, K, mode):
     C = Cbuf[:, :N]
     pad_before = Cbuf[:, N:].clone()
     ref = _lowp_reference(A, B, C, mode)
-    rc = f(A.data_ptr(), K, B.data_ptr(), N, Cbuf.data_ptr(), ldc, M, N, K, mode,
+    # mode 3 (pairs layout) runs on the persistent kernel (148 CTAs)
+    rc = f(A.data_ptr(), K, B.data_ptr(), N, Cbuf.data_ptr(), ldc, M, N, K, mode | ((148 << 8) if mode == 3 else 0),
            torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
     assert rc == 0
     err = (C.double() - ref).abs().max().item()
     # FP32 accumulation of K (3K for the split) products |a b| <= 0.5 * 18.5:
     # a statistical bound 4 u32 K max|a b| (the worst-case bound is K^2 u32 max|ab|)
-    kk = K * (3 if mode == 2 else 1)
+    kk = K * (3 if mode >= 2 else 1)
     assert err <= 4 * 6e-8 * kk * 0.5 * 18.5 + 1e-6, err
     assert torch.equal(Cbuf[:, N:], pad_before)
-    if mode == 2:
+    if mode >= 2:
         # the three-product split reproduces the exact FP32 product to ~u_fp16^2
         split = -_lowp_reference(A, B, torch.zeros_like(C), 2)
         assert (split - A.double() @ B.double()).abs().max().item() <= 1e-5 * 18.5 * K / 64

@@ -6,9 +6,9 @@ Checks: every column of op(A) X = B reaches the scaled residual target
 against the FP64 A (recomputed here in numpy), X agrees with the FP64
 solution, and the adjoint's gradients agree with the FP64 reference
 gradient (lambda = A^{-T} W, grad_A = -lambda X^T) to 1e-10 relative
-(max-norm) when refined to r_hpl < 0.25 (one refinement step past the HPL
-bar of 16, which leaves forward errors near 1e-10 at n = 2048-4096 and
-1e-7 at n = 32768); storing and refactor modes give the same gradient.
+(max-norm) when refined to r_hpl < 1e-3 (the HPL bar of 16 leaves forward
+errors near kappa * n * eps * 16, 1e-10 at n = 2048 and 1e-7 at
+n = 32768); storing and refactor modes give the same gradient.
 References are LAPACK solutions sharpened by one extended-precision
 refinement step."""
 import numpy as np
@@ -117,14 +117,14 @@ def test_refine_adjoint_matches_fp64_gradient(cuda_dev, n, k, b):
     X_ref = _accurate_solve(A, B)
     lam = _accurate_solve(A, W, trans=True)
     gA_ref, gB_ref = -lam @ X_ref.T, lam
-    s = lu.LUSolver(lu.LUConfig(n, b, precision=lu.LU_PREC_FP16X3, ir_target=0.25))
+    s = lu.LUSolver(lu.LUConfig(n, b, precision=lu.LU_PREC_FP16X3, ir_target=1e-3))
     Ad = _padded(A)
     s.refine_factor(Ad)
     X, info = s.refine_apply(Ad, torch.from_numpy(B).cuda())
-    assert info["status"] == 0 and info["r_hpl"] < 0.25
+    assert info["status"] == 0 and info["r_hpl"] < 1e-3
     assert _rel(X.cpu().numpy(), X_ref) < 1e-10
     gA, gB, ai = s.refine_adjoint(Ad, X, torch.from_numpy(W).cuda())
-    assert ai["status"] == 0 and ai["r_hpl"] < 0.25
+    assert ai["status"] == 0 and ai["r_hpl"] < 1e-3
     assert _rel(gB.cpu().numpy(), gB_ref) < 1e-10
     assert _rel(gA.cpu().numpy(), gA_ref) < 1e-10
 
