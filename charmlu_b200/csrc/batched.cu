@@ -127,14 +127,15 @@ template <typename T>
 __device__ int getf2_smem(T* a, int ld, int m, int w, int* piv_s, T* sv, int* sr) {
   int info = 0;
   const int tid = threadIdx.x;
+  // candidate of column 0; later candidates come out of the update pass
+  T bv = 0;
+  int br = -1;
+  for (int i = tid; i < m; i += BT) {
+    const T v = fabs(a[i * ld]);
+    if (v > bv) { bv = v; br = i; }
+  }
   for (int j = 0; j < w && j < m; j++) {
-    T bv = 0;
-    int br = -1;
-    for (int i = j + tid; i < m; i += BT) {
-      const T v = fabs(a[i * ld + j]);
-      if (v > bv) { bv = v; br = i; }
-    }
-    int p = block_argmax(bv, br, sv, sr);
+    int p = block_argmax(bv, br, sv, sr);  // its barriers also end the previous update
     if (p < 0) {
       p = j;
       if (info == 0) info = j + 1;
@@ -147,18 +148,26 @@ __device__ int getf2_smem(T* a, int ld, int m, int w, int* piv_s, T* sv, int* sr
         a[p * ld + c] = t;
       }
     __syncthreads();
+    // one pass per row: multiplier (true division), rank-1 update of the
+    // rest of the block, and the candidate of column j + 1
     const T piv = a[j * ld + j];
-    if (piv != T(0) && !isnan(piv)) {
-      for (int i = j + 1 + tid; i < m; i += BT) a[i * ld + j] = a[i * ld + j] / piv;
-      __syncthreads();
-      const int rw = w - j - 1, rm = m - j - 1;
-      for (int idx = tid; idx < rw * rm; idx += BT) {
-        const int i = j + 1 + idx / rw, c = j + 1 + idx % rw;
-        a[i * ld + c] = fma(-a[i * ld + j], a[j * ld + c], a[i * ld + c]);
+    const bool do_scale = piv != T(0) && !isnan(piv);
+    bv = 0;
+    br = -1;
+    for (int i = j + 1 + tid; i < m; i += BT) {
+      T* ar = a + i * ld;
+      if (do_scale) {
+        const T l = ar[j] / piv;
+        ar[j] = l;
+        for (int c = j + 1; c < w; c++) ar[c] = fma(-l, a[j * ld + c], ar[c]);
+      }
+      if (j + 1 < w) {
+        const T v = fabs(ar[j + 1]);
+        if (v > bv) { bv = v; br = i; }
       }
     }
-    __syncthreads();
   }
+  __syncthreads();
   return info;
 }
 
@@ -241,11 +250,24 @@ __device__ int factor_system(T* A, int n, T* x, int* piv, unsigned char* smem, T
   const int ld = nb + 1;
   T* panel = reinterpret_cast<T*>(smem);                  // n x (nb+1)
   T* ut = panel + (size_t)n * ld;                          // nb x 128
+  __shared__ int sw_dst[64], sw_src[64], sw_m;             // composed row moves of a panel
   for (int k0 = 0; k0 < n; k0 += nb) {
     const int kw = min(nb, n - k0), m = n - k0;
-    for (int idx = tid; idx < m * kw; idx += BT) {
-      const int i = idx / kw, c = idx - i * kw;
-      panel[i * ld + c] = A[(int64_t)(k0 + i) * n + k0 + c];
+    // panel in: eight loads in flight per thread
+    for (int base = 0; base < m * kw; base += BT * 8) {
+      T v[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int idx = base + tid + u * BT;
+        const int i = idx / kw, c = idx - i * kw;
+        v[u] = idx < m * kw ? A[(int64_t)(k0 + i) * n + k0 + c] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int idx = base + tid + u * BT;
+        const int i = idx / kw, c = idx - i * kw;
+        if (idx < m * kw) panel[i * ld + c] = v[u];
+      }
     }
     __syncthreads();
     const int pi = getf2_smem(panel, ld, m, kw, piv_s, sv, sr);
@@ -254,22 +276,59 @@ __device__ int factor_system(T* A, int n, T* x, int* piv, unsigned char* smem, T
       const int i = idx / kw, c = idx - i * kw;
       A[(int64_t)(k0 + i) * n + k0 + c] = panel[i * ld + c];
     }
-    // the panel's swaps on the columns outside it, and on x (in order)
-    for (int j = 0; j < kw; j++) {
-      const int p = piv_s[j];
-      if (tid == 0) piv[k0 + j] = k0 + p;
-      if (p != j) {
-        T* r1 = A + (int64_t)(k0 + j) * n;
-        T* r2 = A + (int64_t)(k0 + p) * n;
-        for (int c = tid; c < n - kw; c += BT) {
-          const int col = c < k0 ? c : c + kw;
-          const T t = r1[col];
-          r1[col] = r2[col];
-          r2[col] = t;
+    // the panel's swaps, in order, composed into one assignment of the
+    // affected rows (row dst <- row src, at most 2 kw moves), then applied to
+    // the columns outside the panel with every source read before any
+    // destination is written; x and the pivot record by thread 0 in order
+    if (tid == 0) {
+      int pos[64], cont[64], np = 0;
+      for (int j = 0; j < kw; j++) {
+        const int p = piv_s[j];
+        piv[k0 + j] = k0 + p;
+        if (p != j) {
+          const T t = x[k0 + j];
+          x[k0 + j] = x[k0 + p];
+          x[k0 + p] = t;
+          int ia = -1, ib = -1;
+          for (int q = 0; q < np; q++) {
+            if (pos[q] == j) ia = q;
+            if (pos[q] == p) ib = q;
+          }
+          if (ia < 0) { pos[np] = j; cont[np] = j; ia = np++; }
+          if (ib < 0) { pos[np] = p; cont[np] = p; ib = np++; }
+          const int t2 = cont[ia];
+          cont[ia] = cont[ib];
+          cont[ib] = t2;
         }
-        if (tid == 0) { const T t = x[k0 + j]; x[k0 + j] = x[k0 + p]; x[k0 + p] = t; }
       }
-      __syncthreads();
+      int mm = 0;
+      for (int q = 0; q < np; q++)
+        if (pos[q] != cont[q]) { sw_dst[mm] = k0 + pos[q]; sw_src[mm] = k0 + cont[q]; mm++; }
+      sw_m = mm;
+    }
+    __syncthreads();
+    {
+      const int mm = sw_m;
+      // four threads per column, each a quarter of the moves (<= 16)
+      const int q4 = tid & 3;
+      for (int cb = 0; cb < n - kw; cb += BT / 4) {
+        const int c = cb + (tid >> 2);
+        const int col = c < k0 ? c : c + kw;
+        const bool live = c < n - kw;
+        T v[16];
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+          const int q = q4 + 4 * u;
+          v[u] = (live && q < mm) ? A[(int64_t)sw_src[q] * n + col] : T(0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+          const int q = q4 + 4 * u;
+          if (live && q < mm) A[(int64_t)sw_dst[q] * n + col] = v[u];
+        }
+        __syncthreads();
+      }
     }
     const int c1 = k0 + kw, nr = n - c1;
     if (nr <= 0) break;
@@ -298,22 +357,36 @@ __device__ int factor_system(T* A, int n, T* x, int* piv, unsigned char* smem, T
     // shared reads and coalesced global read-modify-writes)
     const int tr = tid >> 5, tc = tid & 31;
     for (int ct = c1; ct < n; ct += 128) {
-      for (int idx = tid; idx < kw * 128; idx += BT) {
-        const int p = idx >> 7, c = idx & 127;
-        ut[p * 128 + c] = (ct + c < n) ? A[(int64_t)(k0 + p) * n + ct + c] : T(0);
+      // U12 tile (kw x 128): all of a thread's loads in flight together
+      for (int base = 0; base < kw * 128; base += BT * 8) {
+        T v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int idx = base + tid + u * BT;
+          const int p = idx >> 7, c = idx & 127;
+          v[u] = (idx < kw * 128 && ct + c < n) ? A[(int64_t)(k0 + p) * n + ct + c] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int idx = base + tid + u * BT;
+          if (idx < kw * 128) ut[idx] = v[u];
+        }
       }
       __syncthreads();
-      for (int rt = c1; rt < n; rt += 64) {
-        // C values first (their latency overlaps the FMA loop), then C -= L21 U12
+      T acc[4][4];
+      auto load_c = [&](int rt, T (&dst)[4][4]) {
         const int rbase = rt + tr * 4;
-        T acc[4][4];
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
           for (int j = 0; j < 4; j++) {
             const int r = rbase + i, c = ct + tc + 32 * j;
-            acc[i][j] = (r < n && c < n) ? A[(int64_t)r * n + c] : T(0);
+            dst[i][j] = (r < n && c < n) ? A[(int64_t)r * n + c] : T(0);
           }
+      };
+      load_c(c1, acc);
+      for (int rt = c1; rt < n; rt += 64) {
+        const int rbase = rt + tr * 4;
         for (int p = 0; p < kw; p++) {
           T av[4], bv[4];
 #pragma unroll
@@ -335,6 +408,7 @@ __device__ int factor_system(T* A, int n, T* x, int* piv, unsigned char* smem, T
             if (c < n) A[(int64_t)r * n + c] = acc[i][j];
           }
         }
+        if (rt + 64 < n) load_c(rt + 64, acc);  // the next row tile's C values
       }
       __syncthreads();
     }
