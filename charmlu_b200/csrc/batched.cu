@@ -672,12 +672,11 @@ extern "C" LU_API int lu_batched_factor_solve(int32_t count, const int32_t* n, c
   if (precision != LU_PREC_FP64 && precision != LU_PREC_FP32) return LU_ERR_ARG;
   if (work_bytes < 256 + 20 * (size_t)count) return LU_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(once, [] {
-    attr_err = cudaFuncSetAttribute(batched_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchSmem);
-  });
-  LUB_CUDA(attr_err);
+  static PerDeviceOnce once;
+  LUB_TRY(once_per_device(once, [] {
+    return cuda_status(
+        cudaFuncSetAttribute(batched_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchSmem));
+  }));
   unsigned char* w = static_cast<unsigned char*>(dWork);
   batched_prep_kernel<<<1, 1024, 0, s>>>(count, n, precision, w, (long long)work_bytes, info);
   LUB_LAUNCH_CHECK();

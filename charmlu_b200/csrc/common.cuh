@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <algorithm>
+#include <mutex>
 
 #include "../../include/lu_b200.h"
 
@@ -13,6 +14,33 @@
 #endif
 
 namespace lub {
+
+// Runs f() once per device (the one current when called) for each
+// PerDeviceOnce object and caches its status: kernel attributes such as the
+// dynamic shared-memory limit are per-device state, so one process that
+// drives several GPUs must set them on each.
+struct PerDeviceOnce {
+  std::mutex mu;
+  bool done[64] = {};
+  int status[64] = {};
+};
+template <class F>
+inline int once_per_device(PerDeviceOnce& o, F&& f) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return LU_ERR_CUDA;
+  if (dev < 0 || dev >= 64) return LU_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lk(o.mu);
+  if (!o.done[dev]) {
+    o.status[dev] = f();
+    o.done[dev] = true;
+  }
+  return o.status[dev];
+}
+inline int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return LU_OK;
+  cudaGetLastError();
+  return LU_ERR_CUDA;
+}
 
 constexpr int kNumSMsB200 = 148;
 

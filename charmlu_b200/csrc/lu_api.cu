@@ -62,17 +62,15 @@ int encode_tmap_2d(CUtensorMap* map, CUtensorMapDataType dtype, int elem_bytes, 
 
 long long g_kernel_launches = 0;
 
-static int g_init_status = -1000;
-static std::mutex g_init_mu;
+static PerDeviceOnce g_init;
 int ensure_kernels_init() {
-  std::lock_guard<std::mutex> lk(g_init_mu);
-  if (g_init_status != -1000) return g_init_status;
-  int s = gemm_f64_init();
-  if (s == LU_OK) s = gemm_bf16_init();
-  if (s == LU_OK) s = leaf_init<double>();
-  if (s == LU_OK) s = leaf_init<float>();
-  g_init_status = s;
-  return s;
+  return once_per_device(g_init, [] {
+    int s = gemm_f64_init();
+    if (s == LU_OK) s = gemm_bf16_init();
+    if (s == LU_OK) s = leaf_init<double>();
+    if (s == LU_OK) s = leaf_init<float>();
+    return s;
+  });
 }
 
 }  // namespace lub

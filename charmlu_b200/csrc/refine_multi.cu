@@ -222,12 +222,11 @@ __global__ void col_put_kernel(double* M, int c, const double* v, int n, int ass
 template <bool TRANS, bool NORM>
 int launch_skinny(const double* A, int64_t lda, int n, const double* X, int S, int split_len, double* P, double* Pn,
                   cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    LUB_CUDA(cudaFuncSetAttribute(skinny_residual_kernel<TRANS, NORM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)mr_smem<TRANS>()));
-    attr = true;
-  }
+  static PerDeviceOnce once;
+  LUB_TRY(once_per_device(once, [] {
+    return cuda_status(cudaFuncSetAttribute(skinny_residual_kernel<TRANS, NORM>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mr_smem<TRANS>()));
+  }));
   dim3 grid(ceil_div(n, RB), S);
   skinny_residual_kernel<TRANS, NORM><<<grid, MR_THREADS, mr_smem<TRANS>(), s>>>(A, lda, n, X, split_len, P, Pn);
   LUB_LAUNCH_CHECK();

@@ -450,13 +450,11 @@ __global__ void permute_rows_kernel(const double* X, int64_t ldx, double* Y, int
 
 template <typename TS, int MODE>
 int pipe_attr() {
-  static bool done = false;
-  if (!done) {
-    LUB_CUDA(cudaFuncSetAttribute(trsm_pipe_kernel<TS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)pipe_smem<TS>()));
-    done = true;
-  }
-  return LU_OK;
+  static PerDeviceOnce once;
+  return once_per_device(once, [] {
+    return cuda_status(cudaFuncSetAttribute(trsm_pipe_kernel<TS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)pipe_smem<TS>()));
+  });
 }
 
 template <typename TS>
@@ -522,12 +520,15 @@ int launch_trsv_mixed(const TS* LU, int64_t lda, int n, T* x, int upper, int* fl
   if (n <= 0) return LU_OK;
   const int nblk = ceil_div(n, TB);
   constexpr size_t smem = trsv_smem<TS, T>();
-  static bool attr = false;
-  if (!attr) {
-    LUB_CUDA(cudaFuncSetAttribute(trsv_kernel<TS, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    LUB_CUDA(cudaFuncSetAttribute(trsv_kernel<TS, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
+  static PerDeviceOnce once;
+  LUB_TRY(once_per_device(once, [] {
+    int r = cuda_status(
+        cudaFuncSetAttribute(trsv_kernel<TS, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (r == LU_OK)
+      r = cuda_status(
+          cudaFuncSetAttribute(trsv_kernel<TS, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return r;
+  }));
   // flags[0] is the progress counter; the ticket hands out block order
   LUB_CUDA(cudaMemsetAsync(flags, 0, sizeof(int), s));
   LUB_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), s));
