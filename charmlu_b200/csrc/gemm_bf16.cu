@@ -92,6 +92,21 @@ __device__ __forceinline__ void bulk_wait_read() {
 }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
+// Zero the lanes of a four-column group at or beyond the launch's column
+// count (left = columns remaining from the group's first column). mapB may
+// reach past the launch's N (a narrow update of the next panel's columns
+// inside a wider trailing matrix); those columns belong to another launch and
+// must receive a zero increment from this one.
+__device__ __forceinline__ float4 mask_cols(float4 f, int left) {
+  if (left < 4) {
+    if (left < 1) f.x = 0.f;
+    if (left < 2) f.y = 0.f;
+    if (left < 3) f.z = 0.f;
+    f.w = 0.f;
+  }
+  return f;
+}
+
 struct Bf16GemmArgs {
   int a_row0;   // first row of the tile grid in mapA's matrix (L rows)
   int b_row0;   // first row in mapB's matrix (U^T rows = output columns)
@@ -195,11 +210,12 @@ gemm_bf16_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_const
     if (tid == 0) bulk_wait_read<1>();  // the box written two chunks ago has been read
     __syncthreads();
     unsigned char* box = epi + (c & 1) * EPI_BYTES;
+    const int cols_left = args.N - (tile_n + c * EPI_COLS);
 #pragma unroll
     for (int j = 0; j < 8; j++) {
       float4 f = make_float4(-__uint_as_float(v[4 * j]) * unscale, -__uint_as_float(v[4 * j + 1]) * unscale,
                              -__uint_as_float(v[4 * j + 2]) * unscale, -__uint_as_float(v[4 * j + 3]) * unscale);
-      *reinterpret_cast<float4*>(box + row * 128 + ((j ^ (row & 7)) << 4)) = f;
+      *reinterpret_cast<float4*>(box + row * 128 + ((j ^ (row & 7)) << 4)) = mask_cols(f, cols_left - 4 * j);
     }
     fence_proxy_async();
     __syncthreads();
@@ -388,11 +404,12 @@ gemm_lowp_persistent_kernel(const __grid_constant__ CUtensorMap mapA, const __gr
         if (leader) bulk_wait_read<1>();  // the box written two chunks ago has been read
         epi_bar();
         unsigned char* box = epi + (int)(chunk & 1) * EPI_BYTES;
+        const int cols_left = args.N - (tn * BN + c * EPI_COLS);
 #pragma unroll
         for (int j = 0; j < 8; j++) {
           float4 f = make_float4(-__uint_as_float(v[4 * j]) * unscale, -__uint_as_float(v[4 * j + 1]) * unscale,
                                  -__uint_as_float(v[4 * j + 2]) * unscale, -__uint_as_float(v[4 * j + 3]) * unscale);
-          *reinterpret_cast<float4*>(box + row * 128 + ((j ^ (row & 7)) << 4)) = f;
+          *reinterpret_cast<float4*>(box + row * 128 + ((j ^ (row & 7)) << 4)) = mask_cols(f, cols_left - 4 * j);
         }
         fence_proxy_async();
         epi_bar();
