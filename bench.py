@@ -461,6 +461,76 @@ def run_adjoint(args, rank, world):
     return 0
 
 
+def run_ooc(args, rank, world):
+    """Out-of-core form of the mixed path (lu_refine_solve_host): the FP64
+    matrix stays in pinned host memory. One streamed pass converts it to
+    FP32; its leading rows stay in HBM as far as they fit beside the FP32
+    factors, and each refinement step's FP64 residual streams only the rest.
+    At N=65536 it is timed with all rows resident and with none (every
+    residual streams the whole matrix), beside the device-resident solve of
+    the same matrix (same x bit for bit); --ooc-n above ~115k takes orders
+    whose FP64 matrix does not fit in HBM beside the factors."""
+    import torch
+    import charmlu_b200 as lu
+    if rank != 0:
+        return 0
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    rows = []
+    cases = [(65536, None), (65536, 0)] + ([(args.ooc_n, None)] if args.ooc_n != 65536 else [])
+    for n, resident in cases:
+        if resident is None:
+            os.environ.pop("LU_B200_RESIDENT_BYTES", None)
+        else:
+            os.environ["LU_B200_RESIDENT_BYTES"] = str(resident)
+        need = 8 * n * n
+        try:
+            import psutil
+            avail = psutil.virtual_memory().available
+        except Exception:
+            avail = 0
+        if avail < 1.15 * need:
+            rows.append({"n": n, "skipped": f"host memory {avail / 1e9:.0f} GB < {1.15 * need / 1e9:.0f} GB"})
+            print(json.dumps(rows[-1]), flush=True)
+            continue
+        hA = torch.empty(n, n, dtype=torch.float64, pin_memory=True)
+        chunk = max(1, (1 << 30) // (8 * n))  # rows per 1 GiB generated on the device
+        for r0 in range(0, n, chunk):
+            r = min(chunk, n - r0)
+            hA[r0:r0 + r].copy_(lu.generate_uniform(r, n, seed=42, stream_id=1000 + r0 // chunk, device=dev))
+        b = lu.generate_uniform(n, 1, seed=42, stream_id=1, device=dev).view(-1)
+        s = lu.LUSolver(lu.LUConfig(n, args.block_mixed, precision=lu.LU_PREC_FP16X3, lookahead=True))
+        x = torch.empty_like(b)
+        s.refine_solve_host(hA, b, x)  # warm (staging, resident rows and workspace allocation)
+        ms = []
+        for _ in range(max(1, args.steps - 1)):
+            (_, info), t = _timed(lambda: s.refine_solve_host(hA, b, x))
+            ms.append(t)
+        t = sum(ms) / len(ms)
+        row = {"n": n, "resident_rows": "all that fit in HBM" if resident is None else f"at most {resident} bytes",
+               "ms": t, "tflops": flops_lu(n) / (t / 1e3) / 1e12, "status": s.status(), "r_hpl": info["r_hpl"],
+               "ir_iterations": info["iterations"], "gmres_iterations": info["gmres_iterations"],
+               "host_to_device_bytes_per_solve": info["host_bytes"],
+               "host_to_device_gb_per_s_over_solve": info["host_bytes"] / (t / 1e3) / 1e9,
+               "fp32_factors_gb_on_device": 4 * n * n / 1e9, "fp64_matrix_gb_in_host_memory": 8 * n * n / 1e9}
+        if resident is None and 8 * n * n * 1.6 < torch.cuda.mem_get_info(dev)[0]:
+            dA = hA.to(dev)
+            xd = torch.empty_like(b)
+            s2 = lu.LUSolver(lu.LUConfig(n, args.block_mixed, precision=lu.LU_PREC_FP16X3, lookahead=True))
+            s2.refine_solve(dA, b, xd)
+            (_, _), td = _timed(lambda: s2.refine_solve(dA, b, xd))
+            row["device_resident_ms"] = td
+            row["same_x_as_device_resident"] = bool(torch.equal(x, xd))
+            del dA, s2
+        rows.append(row)
+        print(json.dumps(row), flush=True)
+        del hA, s
+        torch.cuda.empty_cache()
+    os.environ.pop("LU_B200_RESIDENT_BYTES", None)
+    print(json.dumps({"metric": "out-of-core mixed solve: FP64 A in host memory", "rows": rows}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -479,7 +549,8 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=8192)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="lu", choices=["lu", "batched", "ksweep", "adjoint"])
+    ap.add_argument("--workload", default="lu", choices=["lu", "batched", "ksweep", "adjoint", "ooc"])
+    ap.add_argument("--ooc-n", type=int, default=65536)
     ap.add_argument("--adjoint-n", type=int, default=4096)
     ap.add_argument("--adjoint-mixed-n", type=int, default=32768)
     ap.add_argument("--adjoint-target", type=float, default=1e-3)
@@ -499,6 +570,8 @@ def main():
         return run_ksweep(args, rank, world)
     if args.workload == "adjoint":
         return run_adjoint(args, rank, world)
+    if args.workload == "ooc":
+        return run_ooc(args, rank, world)
 
     import torch
     import charmlu_b200 as lu

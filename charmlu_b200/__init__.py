@@ -230,6 +230,24 @@ class LUSolver:
                                        _stream(stream)), "lu_refine_solve")
         return x, {k: getattr(info, k) for k, _ in info._fields_}
 
+    def refine_solve_host(self, A_host, b, x=None, stream=None):
+        """refine_solve with the FP64 matrix in host memory (CPU tensor,
+        pinned for full copy speed; lu_refine_solve_host). Its leading rows
+        stay in HBM as far as they fit beside the FP32 factors; each pass over
+        A streams the others in row chunks. info["host_bytes"] counts the
+        bytes copied."""
+        if not isinstance(A_host, torch.Tensor) or A_host.device.type != "cpu" or A_host.dtype != torch.float64:
+            raise LUError(LU_ERR_ARG, "A_host must be a float64 CPU tensor")
+        n = self.n
+        if A_host.dim() != 2 or A_host.shape[0] != n or A_host.shape[1] != n or A_host.stride(1) != 1:
+            raise LUError(LU_ERR_ARG, "A_host must be n x n with unit column stride")
+        _require_cuda(b, torch.float64, "b")
+        if x is None:
+            x = torch.empty_like(b)
+        info = _lib.LuRefineInfo()
+        _check(self._L.lu_refine_solve_host(self._h, _ptr(A_host), A_host.stride(0), _ptr(b), _ptr(x),
+                                            ctypes.byref(info), _stream(stream)), "lu_refine_solve_host")
+        return x, {k: getattr(info, k) for k, _ in info._fields_}
 
     def refine_factor(self, A, stream=None):
         """Low-precision factorisation of A kept in the handle for

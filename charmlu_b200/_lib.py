@@ -18,7 +18,7 @@ LU_IR_CLASSIC, LU_IR_GMRES = 0, 1
 # every symbol the header declares (checked by the CPU test suite)
 EXPORTS = [
     "lu_config_default", "lu_create", "lu_destroy", "lu_workspace_bytes", "lu_status", "lu_factor",
-    "lu_solve", "lu_factor_solve", "lu_residual", "lu_refine_solve", "lu_adjoint",
+    "lu_solve", "lu_factor_solve", "lu_residual", "lu_refine_solve", "lu_refine_solve_host", "lu_adjoint",
     "lu_batched_factor_solve", "lu_generate_uniform", "lu_matgen_host", "lu_status_string",
     "lu_profile", "lu_phase_times", "lu_launch_count", "lu_solve_noalloc",
     "lu_batched_work_bytes", "lu_batched_set_tuning", "lu_refine_factor", "lu_refine_apply",
@@ -43,7 +43,7 @@ class LuResidualInfo(ctypes.Structure):
 class LuRefineInfo(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int32), ("gmres_iterations", ctypes.c_int32),
                 ("used_gmres", ctypes.c_int32), ("status", ctypes.c_int32),
-                ("r_hpl", ctypes.c_double), ("r_hpl_initial", ctypes.c_double)]
+                ("r_hpl", ctypes.c_double), ("r_hpl_initial", ctypes.c_double), ("host_bytes", ctypes.c_int64)]
 
 
 _lib = None
@@ -70,6 +70,7 @@ def load():
         "lu_factor_solve": ([H, P, i64, P, P, P], ctypes.c_int),
         "lu_residual": ([H, P, i64, P, P, ctypes.POINTER(LuResidualInfo), P], ctypes.c_int),
         "lu_refine_solve": ([H, P, i64, P, P, ctypes.POINTER(LuRefineInfo), P], ctypes.c_int),
+        "lu_refine_solve_host": ([H, P, i64, P, P, ctypes.POINTER(LuRefineInfo), P], ctypes.c_int),
         "lu_adjoint": ([H, P, i64, P, P, i64, P, i64, i64, P, i64, P, i64, P], ctypes.c_int),
         "lu_refine_factor": ([H, P, i64, P], ctypes.c_int),
         "lu_refine_apply": ([H, P, i64, i32, P, i64, P, i64, i64, ctypes.POINTER(LuRefineInfo), P], ctypes.c_int),

@@ -2,6 +2,7 @@
 // shared by the FP64 and mixed-precision orchestration.
 #pragma once
 #include <cuda_bf16.h>
+#include <algorithm>
 #include <vector>
 
 #include "common.cuh"
@@ -97,6 +98,23 @@ struct lu_handle_s {
   double* mr_T = nullptr;      // GMRES: product block
   double* mr_dc = nullptr;     // GMRES: correction of one column
   unsigned long long* mr_acc = nullptr;
+  // host-resident FP64 A (lu_refine_solve_host): row chunks staged through
+  // two device buffers, copies on sCopy overlapping the kernels on the
+  // caller's stream
+  double* stage[2] = {nullptr, nullptr};
+  int64_t stage_elems = 0;
+  size_t stage_bytes = size_t(256) << 20;  // per buffer
+  cudaStream_t sCopy = nullptr;
+  cudaEvent_t evReady[2] = {nullptr, nullptr}, evFree[2] = {nullptr, nullptr};
+  // leading rows of the host matrix kept in device memory (as many as free
+  // memory allows, at most resident_cap bytes): the conversion pass of every
+  // call copies them there, and each later pass over A (residuals, GMRES
+  // products) streams only rows res_rows .. n-1
+  double* resA = nullptr;
+  int64_t res_elems = 0;
+  int res_rows = 0;
+  size_t resident_cap = ~size_t(0);
+  int64_t host_copied = 0;  // bytes of host A copied to the device, running total
   std::vector<void*> allocs;
   size_t bytes = 0;
   long long spin = 0;
@@ -143,6 +161,11 @@ struct lu_handle_s {
     bytes += count * sizeof(T);
     *p = static_cast<T*>(q);
     return LU_OK;
+  }
+  void release(void* p) {
+    if (!p) return;
+    cudaFree(p);
+    allocs.erase(std::remove(allocs.begin(), allocs.end(), p), allocs.end());
   }
   unsigned* take_counter() {
     if (next_counter >= n_counters) return nullptr;

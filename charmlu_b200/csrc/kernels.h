@@ -110,6 +110,10 @@ struct ResidualAccum {  // non-negative doubles stored as ordered bit patterns
 };
 int launch_residual_f64(const double* A, int64_t lda, int n, const double* x, const double* b, double* r,
                         ResidualAccum* acc, cudaStream_t s);
+// the same for rows row0 .. row0 + rows - 1 only (Arows = their first row);
+// accumulates into acc without clearing it
+int launch_residual_f64_rows(const double* Arows, int64_t lda, int rows, int row0, int n, const double* x,
+                             const double* b, double* r, ResidualAccum* acc, cudaStream_t s);
 // factors stored as TS, vector and arithmetic in T (FP32 factors, FP64 vector)
 template <typename TS, typename T>
 int launch_trsv_mixed(const TS* LU, int64_t lda, int n, T* x, int upper, int* flags, unsigned* ticket, DevStatus* st,

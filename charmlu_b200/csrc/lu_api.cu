@@ -321,6 +321,8 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
   if (const char* e = getenv("LU_B200_LEAF_W32_LA")) h->leaf_w32_la = std::min(64, std::max(4, atoi(e)));
   if (const char* e = getenv("LU_B200_GEMM_CTAS")) h->gemm_ctas = std::max(0, atoi(e));
   if (const char* e = getenv("LU_B200_GEMM_RESERVE")) h->gemm_reserve = std::max(0, atoi(e));
+  if (const char* e = getenv("LU_B200_STAGE_BYTES")) h->stage_bytes = std::max<size_t>(1 << 16, strtoull(e, nullptr, 10));
+  if (const char* e = getenv("LU_B200_RESIDENT_BYTES")) h->resident_cap = strtoull(e, nullptr, 10);
   if (s == LU_OK) s = h->alloc(&h->perm, n);
   if (s == LU_OK) s = h->alloc(&h->perm_work, n);
   if (s == LU_OK) s = h->alloc(&h->perm_lists, lub::ipiv_to_perm_work_ints((int)n));
@@ -351,6 +353,11 @@ int lu_destroy(lu_handle h) {
   if (h->evG0) cudaEventDestroy(h->evG0);
   if (h->evG1) cudaEventDestroy(h->evG1);
   if (h->sG) cudaStreamDestroy(h->sG);
+  for (int b = 0; b < 2; b++) {
+    if (h->evReady[b]) cudaEventDestroy(h->evReady[b]);
+    if (h->evFree[b]) cudaEventDestroy(h->evFree[b]);
+  }
+  if (h->sCopy) cudaStreamDestroy(h->sCopy);
   for (void* p : h->allocs) cudaFree(p);
   if (h->racc_host) cudaFreeHost(h->racc_host);
   delete h;

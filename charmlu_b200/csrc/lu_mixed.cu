@@ -251,13 +251,105 @@ double bits_to_double(unsigned long long v) {
   return x;
 }
 
+// The FP64 matrix the mixed path reads (conversion, residuals, GMRES
+// products): in device memory, or in host memory (host = true) and passed
+// through the GPU row by row.
+struct ASrc {
+  const double* A;
+  int64_t lda;
+  bool host;
+};
+
+int ensure_staging(lu_handle h, int64_t lda) {
+  const int64_t rows = std::max<int64_t>(1, (int64_t)(h->stage_bytes / sizeof(double)) / lda);
+  const int64_t need = rows * lda;
+  if (h->stage[0] && h->stage_elems >= need) return LU_OK;
+  for (int b = 0; b < 2; b++) {
+    h->release(h->stage[b]);
+    h->stage[b] = nullptr;
+    LUB_TRY(h->alloc(&h->stage[b], (size_t)need));
+    if (!h->evReady[b]) LUB_CUDA(cudaEventCreateWithFlags(&h->evReady[b], cudaEventDisableTiming));
+    if (!h->evFree[b]) LUB_CUDA(cudaEventCreateWithFlags(&h->evFree[b], cudaEventDisableTiming));
+  }
+  if (!h->sCopy) LUB_CUDA(cudaStreamCreateWithFlags(&h->sCopy, cudaStreamNonBlocking));
+  h->stage_elems = need;
+  return LU_OK;
+}
+
+// Sizes the device copy of the host matrix's leading rows: every row that
+// fits in free device memory less a margin (2 GB or 1/32 of the device, for
+// the refinement's later buffers), at most h->resident_cap bytes. The
+// current copy counts as free, since it is replaced. Sets h->res_rows.
+int ensure_resident(lu_handle h, int64_t lda, int n) {
+  size_t free_b = 0, total_b = 0;
+  LUB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const size_t have = (size_t)h->res_elems * sizeof(double);
+  const size_t margin = std::max<size_t>(size_t(2) << 30, total_b / 32);
+  size_t budget = free_b + have > margin ? free_b + have - margin : 0;
+  budget = std::min(budget, h->resident_cap);
+  int64_t rows = std::min<int64_t>(n, (int64_t)(budget / (sizeof(double) * (size_t)lda)));
+  h->res_rows = 0;
+  if (rows <= 0) return LU_OK;
+  if (h->res_elems < rows * lda) {
+    h->release(h->resA);
+    h->resA = nullptr;
+    h->res_elems = 0;
+    // a failed allocation (fragmentation) halves the request
+    while (rows > 0 && h->alloc(&h->resA, (size_t)(rows * lda)) != LU_OK) rows /= 2;
+    if (rows <= 0) return LU_OK;
+    h->res_elems = rows * lda;
+  }
+  h->res_rows = (int)rows;
+  return LU_OK;
+}
+
+// One pass over the rows of the host matrix. Rows below h->res_rows are
+// copied into h->resA when fill is set (the conversion pass) and read there
+// in place otherwise; the other rows pass in chunks through the two staging
+// buffers. Copies run on h->sCopy and overlap the kernels that
+// f(rows_dev, row0, rows) launches on s; rows_dev has pitch lda.
+template <class F>
+int stream_host_rows(lu_handle h, const double* hA, int64_t lda, int n, bool fill, cudaStream_t s, F f) {
+  LUB_TRY(ensure_staging(h, lda));
+  const int R = (int)std::min<int64_t>(n, h->stage_elems / lda);
+  const int nres = h->res_rows;
+  for (int b = 0; b < 2; b++) LUB_CUDA(cudaEventRecord(h->evFree[b], s));
+  if (!fill && nres > 0) LUB_TRY(f(static_cast<const double*>(h->resA), 0, nres));
+  for (int c = fill ? 0 : nres, k = 0; c < n; k++) {
+    const int b = k & 1;
+    const bool res = c < nres;
+    const int rows = std::min(R, (res ? nres : n) - c);
+    double* dst = res ? h->resA + (int64_t)c * lda : h->stage[b];
+    LUB_CUDA(cudaStreamWaitEvent(h->sCopy, h->evFree[b], 0));  // earlier readers of dst on s are done
+    LUB_CUDA(cudaMemcpyAsync(dst, hA + (int64_t)c * lda, sizeof(double) * (size_t)rows * lda,
+                             cudaMemcpyHostToDevice, h->sCopy));
+    h->host_copied += (int64_t)sizeof(double) * rows * lda;
+    LUB_CUDA(cudaEventRecord(h->evReady[b], h->sCopy));
+    LUB_CUDA(cudaStreamWaitEvent(s, h->evReady[b], 0));
+    LUB_TRY(f(static_cast<const double*>(dst), c, rows));
+    if (!res) LUB_CUDA(cudaEventRecord(h->evFree[b], s));
+    c += rows;
+  }
+  return LU_OK;
+}
+
+// r = b - A x with the norms in h->racc (cleared first)
+int residual_src(lu_handle h, const ASrc& a, const double* x, const double* b, double* r, cudaStream_t s) {
+  const int n = (int)h->cfg.n;
+  if (!a.host) return launch_residual_f64(a.A, a.lda, n, x, b, r, h->racc, s);
+  LUB_CUDA(cudaMemsetAsync(h->racc, 0, sizeof(ResidualAccum), s));
+  return stream_host_rows(h, a.A, a.lda, n, false, s, [&](const double* rows_dev, int r0, int rows) {
+    return launch_residual_f64_rows(rows_dev, a.lda, rows, r0, n, x, b, r, h->racc, s);
+  });
+}
+
 // r = b - A x, its norms, and r_hpl (synchronises).
-int residual_hpl(lu_handle h, const double* A, int64_t lda, const double* x, const double* b, double* r,
-                 double* r_hpl, double* rnorm, cudaStream_t s) {
+int residual_hpl(lu_handle h, const ASrc& A, const double* x, const double* b, double* r, double* r_hpl,
+                 double* rnorm, cudaStream_t s) {
   const int n = (int)h->cfg.n;
   {
     Prof pf(h, s, LU_PH_OTHER);
-    LUB_TRY(launch_residual_f64(A, lda, n, x, b, r, h->racc, s));
+    LUB_TRY(residual_src(h, A, x, b, r, s));
   }
   LUB_CUDA(cudaMemcpyAsync(h->racc_host, h->racc, sizeof(ResidualAccum), cudaMemcpyDeviceToHost, s));
   LUB_CUDA(cudaStreamSynchronize(s));
@@ -355,8 +447,7 @@ int gmres_cycle(lu_handle h, double* x, double rnorm, cudaStream_t s, int* iters
 
 // GMRES cycle of the single-RHS solve A x = b (residual in h->r64, its
 // norms in h->racc)
-int gmres_correction(lu_handle h, const double* A, int64_t lda, double* x, double rnorm, cudaStream_t s,
-                     int* iters_out) {
+int gmres_correction(lu_handle h, const ASrc& A, double* x, double rnorm, cudaStream_t s, int* iters_out) {
   const int n = (int)h->cfg.n;
   auto init = [&](double* v0) {
     LUB_TRY(launch_gather_f64(h->r64, h->perm, v0, n, 1.0, h->racc, s));
@@ -365,7 +456,7 @@ int gmres_correction(lu_handle h, const double* A, int64_t lda, double* x, doubl
   auto op_prec = [&](const double* vj, double* w) {
     {  // residual kernel with b = 0 gives -A v_j
       Prof pf(h, s, LU_PH_OTHER);
-      LUB_TRY(launch_residual_f64(A, lda, n, vj, h->zero64, h->z64, h->racc, s));
+      LUB_TRY(residual_src(h, A, vj, h->zero64, h->z64, s));
     }
     LUB_TRY(launch_gather_f64(h->z64, h->perm, w, n, -1.0, nullptr, s));
     return solve_f32_factors_f64(h, w, s);
@@ -388,11 +479,33 @@ int mixed_factor(lu_handle h, const double* A, int64_t lda, cudaStream_t s) {
   });
 }
 
-int refine_solve(lu_handle h, const double* A, int64_t lda, const double* b, double* x, lu_refine_info* info,
-                 cudaStream_t s) {
+// The host matrix in FP32 into h->A32 (the device copy of its leading rows
+// refreshed on the way), then the low-precision factorisation. No graph
+// replay: the copies depend on the caller's host pointer.
+int mixed_factor_host(lu_handle h, const ASrc& a, cudaStream_t s) {
   const int n = (int)h->cfg.n;
+  LUB_TRY(ensure_mixed(h));
+  LUB_CUDA(cudaMemsetAsync(h->st, 0, sizeof(DevStatus), s));
+  LUB_TRY(ensure_staging(h, a.lda));
+  LUB_TRY(ensure_resident(h, a.lda, n));
+  {
+    Prof pf(h, s, LU_PH_OTHER);
+    LUB_TRY(stream_host_rows(h, a.A, a.lda, n, true, s, [&](const double* rows_dev, int r0, int rows) {
+      return launch_f64_to_f32(rows_dev, a.lda, h->A32 + (int64_t)r0 * h->ld32, h->ld32, rows, n, s);
+    }));
+  }
+  return factor_mixed(h, s);
+}
+
+int refine_solve(lu_handle h, const ASrc& A, const double* b, double* x, lu_refine_info* info, cudaStream_t s) {
+  const int n = (int)h->cfg.n;
+  const int64_t copied0 = h->host_copied;
   h->mixed_factored = false;
-  LUB_TRY(mixed_factor(h, A, lda, s));
+  if (A.host) {
+    LUB_TRY(mixed_factor_host(h, A, s));
+  } else {
+    LUB_TRY(mixed_factor(h, A.A, A.lda, s));
+  }
   // x0 = U^{-1} L^{-1} P b in FP32
   LUB_TRY(launch_gather_f64_to_f32(b, h->perm, h->v32, n, 1.0, s));
   LUB_TRY(solve32(h, h->v32, s));
@@ -402,6 +515,7 @@ int refine_solve(lu_handle h, const double* A, int64_t lda, const double* b, dou
   memset(&ri, 0, sizeof(ri));
   if (fst != LU_OK) {
     ri.status = fst;
+    ri.host_bytes = h->host_copied - copied0;
     if (info) *info = ri;
     return LU_OK;  // numerical status is reported through lu_status / info
   }
@@ -411,7 +525,7 @@ int refine_solve(lu_handle h, const double* A, int64_t lda, const double* b, dou
   double prev = INFINITY, r_hpl = INFINITY, rn = 0.0;
   int it = 0, gm_stall = 0;
   for (; it < max_it; it++) {
-    LUB_TRY(residual_hpl(h, A, lda, x, b, h->r64, &r_hpl, &rn, s));
+    LUB_TRY(residual_hpl(h, A, x, b, h->r64, &r_hpl, &rn, s));
     if (it == 0) ri.r_hpl_initial = r_hpl;
     if (!std::isfinite(r_hpl)) break;
     if (r_hpl < target) break;
@@ -423,7 +537,7 @@ int refine_solve(lu_handle h, const double* A, int64_t lda, const double* b, dou
     prev = r_hpl;
     if (gm) {
       int k = 0;
-      LUB_TRY(gmres_correction(h, A, lda, x, rn, s, &k));
+      LUB_TRY(gmres_correction(h, A, x, rn, s, &k));
       ri.used_gmres = 1;
       ri.gmres_iterations += k;
     } else {
@@ -439,6 +553,7 @@ int refine_solve(lu_handle h, const double* A, int64_t lda, const double* b, dou
     int code = ri.status;
     LUB_CUDA(cudaMemcpyAsync(&h->st->code, &code, sizeof(int), cudaMemcpyHostToDevice, s));
   }
+  ri.host_bytes = h->host_copied - copied0;
   if (info) *info = ri;
   return LU_OK;
 }
@@ -680,5 +795,20 @@ extern "C" int lu_refine_solve(lu_handle h, const double* dA, int64_t lda, const
   if (h->cfg.precision == LU_PREC_FP64) return LU_ERR_UNSUPPORTED;
   if (h->cfg.block_size % 64) return LU_ERR_ARG;  // whole 64-wide BF16 k-blocks per panel
   LUB_TRY(ensure_kernels_init());
-  return refine_solve(h, dA, lda, db, dx, info, (cudaStream_t)stream);
+  return refine_solve(h, ASrc{dA, lda, false}, db, dx, info, (cudaStream_t)stream);
+}
+
+extern "C" int lu_refine_solve_host(lu_handle h, const double* hA, int64_t lda, const double* db, double* dx,
+                                    lu_refine_info* info, void* stream) {
+  if (!h || !hA || !db || !dx || lda < h->cfg.n) return LU_ERR_ARG;
+  if (h->cfg.precision == LU_PREC_FP64 || h->cfg.precision == LU_PREC_FP32) return LU_ERR_UNSUPPORTED;
+  if (h->cfg.block_size % 64) return LU_ERR_ARG;
+  cudaPointerAttributes pa;
+  if (cudaPointerGetAttributes(&pa, hA) != cudaSuccess) {
+    cudaGetLastError();
+    return LU_ERR_ARG;
+  }
+  if (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged) return LU_ERR_ARG;  // lu_refine_solve
+  LUB_TRY(ensure_kernels_init());
+  return refine_solve(h, ASrc{hA, lda, true}, db, dx, info, (cudaStream_t)stream);
 }

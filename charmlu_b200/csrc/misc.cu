@@ -14,14 +14,18 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* p, double 
   atomicMax(p, (unsigned long long)__double_as_longlong(v));
 }
 
-__global__ void __launch_bounds__(256) residual_f64_kernel(const double* A, int64_t lda, int n, const double* x,
-                                                           const double* b, double* r, ResidualAccum* acc) {
+// Rows row0 .. row0 + rows - 1 of the system; A points at row row0 (a
+// device-resident matrix, or a chunk of a host matrix staged on the device).
+__global__ void __launch_bounds__(256) residual_f64_kernel(const double* A, int64_t lda, int rows, int row0, int n,
+                                                           const double* x, const double* b, double* r,
+                                                           ResidualAccum* acc) {
   __shared__ double s_m[8], s_rs[8], s_r[8], s_b[8], s_x[8];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row = blockIdx.x * 8 + warp;
+  const int lrow = blockIdx.x * 8 + warp;
+  const int row = row0 + lrow;
   double m = 0.0, rs = 0.0, ra = 0.0, bb = 0.0, xx = 0.0;
-  if (row < n) {
-    const double* ar = A + (int64_t)row * lda;
+  if (lrow < rows) {
+    const double* ar = A + (int64_t)lrow * lda;
     double s0 = 0.0, s1 = 0.0;
     const bool vec = ((lda & 1) == 0) && ((reinterpret_cast<uintptr_t>(A) & 15) == 0);
     if (vec) {
@@ -108,7 +112,15 @@ int launch_residual_f64(const double* A, int64_t lda, int n, const double* x, co
                         ResidualAccum* acc, cudaStream_t s) {
   LUB_CUDA(cudaMemsetAsync(acc, 0, sizeof(ResidualAccum), s));
   if (n <= 0) return LU_OK;
-  residual_f64_kernel<<<ceil_div(n, 8), 256, 0, s>>>(A, lda, n, x, b, r, acc);
+  residual_f64_kernel<<<ceil_div(n, 8), 256, 0, s>>>(A, lda, n, 0, n, x, b, r, acc);
+  LUB_LAUNCH_CHECK();
+  return LU_OK;
+}
+
+int launch_residual_f64_rows(const double* Arows, int64_t lda, int rows, int row0, int n, const double* x,
+                             const double* b, double* r, ResidualAccum* acc, cudaStream_t s) {
+  if (rows <= 0) return LU_OK;
+  residual_f64_kernel<<<ceil_div(rows, 8), 256, 0, s>>>(Arows, lda, rows, row0, n, x, b, r, acc);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }

@@ -107,6 +107,7 @@ typedef struct lu_refine_info {
   int32_t status;            /* LU_OK or LU_ERR_NOCONV */
   double  r_hpl;             /* final scaled residual */
   double  r_hpl_initial;     /* scaled residual of the low-precision solve */
+  int64_t host_bytes;        /* bytes of A copied host -> device (lu_refine_solve_host; else 0) */
 } lu_refine_info;
 
 /* Fill *cfg with defaults for order n and block size b (LUConfig defaults,
@@ -158,6 +159,23 @@ LU_API int lu_residual(lu_handle h, const double* dA, int64_t lda, const double*
  * fallback).  dA is read only; db is read only; dx receives x. */
 LU_API int lu_refine_solve(lu_handle h, const double* dA, int64_t lda, const double* db, double* dx,
                     lu_refine_info* info, void* stream);
+
+/* lu_refine_solve with the FP64 matrix in host memory (no reference
+ * counterpart; the out-of-core form of the mixed path, for orders whose FP64
+ * matrix does not fit in HBM beside the FP32 factors).  hA (n x n,
+ * row-major, lda; page-locked memory for full copy speed) is read only.
+ * One pass converts it to the FP32 working copy; its leading rows stay in
+ * device memory (as many as fit beside the factors, less a margin; at most
+ * LU_B200_RESIDENT_BYTES bytes when that variable is set at lu_create), and
+ * every later pass over A (the FP64 residual of each refinement step, each
+ * GMRES product) reads those in place and streams only the other rows
+ * through two staging buffers (LU_B200_STAGE_BYTES each, 256 MB default),
+ * the copies overlapping the kernels.  info->host_bytes counts the bytes
+ * copied.  db, dx and the result are as in lu_refine_solve (the same
+ * arithmetic: the same x bit for bit).  A device pointer for hA is
+ * rejected (LU_ERR_ARG). */
+LU_API int lu_refine_solve_host(lu_handle h, const double* hA, int64_t lda, const double* db, double* dx,
+                         lu_refine_info* info, void* stream);
 
 /* Low-precision factorisation kept in the handle (no reference
  * counterpart): dA (read only) is converted to FP32 and factored as in

@@ -160,10 +160,14 @@ def test_singular_matrix_reports_info_mixed(cuda_dev):
     assert st == 101, (st, info)
 
 
-@pytest.mark.parametrize("n,b", [(2048, 256), (4096, 512)])
+@pytest.mark.parametrize("n,b", [(2048, 256), (4096, 512), (1500, 192), (1000, 64), (2000, 320)])
 def test_refine_lookahead(cuda_dev, n, b):
+    """Block sizes that are not a multiple of the 256-column update tile make
+    the next-panel update's last tile reach into columns the rest update
+    owns; those must receive a zero increment from it."""
     s, A, rhs, x, info, st = _refine(n, b, lookahead=True)
     assert st == 0 and info["status"] == 0, info
+    assert info["used_gmres"] == 0 and info["iterations"] <= 4, info
     assert s.residual(A, x, rhs)["r_hpl"] < 16
 
 
@@ -212,3 +216,38 @@ def test_refine_graph_replay(cuda_dev):
         _, info = sg.refine_solve(A, rhs, x)
         assert sg.status() == 0 and info["status"] == 0
         assert torch.equal(x, x0)
+
+
+@pytest.mark.parametrize("n,b,stage,resident", [(1500, 192, 1 << 20, 0), (2048, 256, 3 << 20, 11 << 20),
+                                                (3000, 256, 5 << 20, 1 << 20), (8192, 512, 0, None)])
+def test_refine_solve_host_matches_device(cuda_dev, n, b, stage, resident, monkeypatch):
+    """The mixed path with the FP64 matrix in host memory gives the
+    device-resident path's x bit for bit. Leading rows up to `resident`
+    bytes stay on the device (0: none, every pass streams all rows; None:
+    all that fit); the others stream in row chunks (small chunks force many
+    double-buffered copies; 0 keeps the 256 MB default)."""
+    import charmlu_b200 as lu
+    if stage:
+        monkeypatch.setenv("LU_B200_STAGE_BYTES", str(stage))
+    if resident is not None:
+        monkeypatch.setenv("LU_B200_RESIDENT_BYTES", str(resident))
+    A = lu.generate_uniform(n, n, seed=77, stream_id=0)
+    bvec = lu.generate_uniform(n, 1, seed=77, stream_id=1).view(-1)
+    s = lu.LUSolver(lu.LUConfig(n, b, precision=lu.LU_PREC_FP16X3, lookahead=True))
+    x_dev, i_dev = s.refine_solve(A, bvec)
+    hA = A.cpu().pin_memory()
+    x_host, i_host = s.refine_solve_host(hA, bvec)
+    torch.cuda.synchronize()
+    assert i_host["status"] == 0 and i_host["r_hpl"] < 16, i_host
+    assert i_host["iterations"] == i_dev["iterations"]
+    assert torch.equal(x_host, x_dev)
+    # one full pass (the conversion), then only the non-resident rows per residual
+    lda = hA.stride(0)
+    rows = n if resident is None else min(n, resident // (8 * lda))
+    assert i_dev["host_bytes"] == 0 and i_host["used_gmres"] == 0
+    assert i_host["host_bytes"] == 8 * lda * (n + (n - rows) * (i_host["iterations"] + 1))
+    # a second call on the same handle reuses the staging and resident buffers
+    x2, i2 = s.refine_solve_host(hA, bvec)
+    assert torch.equal(x2, x_dev) and i2["host_bytes"] == i_host["host_bytes"]
+    with pytest.raises(lu.LUError):
+        s.refine_solve_host(A, bvec)  # a device tensor is rejected
