@@ -117,6 +117,7 @@ struct Bf16GemmArgs {
   DevStatus* st;
   long long spin;
   int kpart;    // pairs layout: element offset of the lo parts (K = kpart); 0 otherwise
+  unsigned* tile_ctr;  // persistent kernel: shared tile counter (dynamic tiles) or null (static striding)
 };
 
 __global__ void __launch_bounds__(THREADS, 1)
@@ -272,6 +273,12 @@ gemm_lowp_persistent_kernel(const __grid_constant__ CUtensorMap mapA, const __gr
   uint64_t* tempty = tfull + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
   __shared__ int s_epi_fail;  // sticky: the epilogue warps stop together
+  // The producer picks each tile (from the shared counter, or by striding)
+  // and publishes it here for the MMA warp and the epilogue: entry i & 7
+  // holds this CTA's i-th tile, -1 once there are no more.  The producer runs
+  // at most 2 tiles + one ring of k-blocks ahead of the epilogue, so an entry
+  // is read before it is reused.
+  __shared__ volatile int s_tiles[8];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ntm = (args.M + BM - 1) / BM, ntn = (args.N + BN - 1) / BN;
@@ -309,7 +316,19 @@ gemm_lowp_persistent_kernel(const __grid_constant__ CUtensorMap mapA, const __gr
     if (lane == 0) {  // ---- TMA producer
       long long kb = 0;
       bool ok = true;
-      for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+      for (int i = 0; ok; i++) {
+        int t = args.tile_ctr ? (int)atomicAdd(args.tile_ctr, 1u) : (int)blockIdx.x + i * (int)gridDim.x;
+        if (t >= tiles) t = -1;
+        s_tiles[i & 7] = t;
+        __threadfence_block();
+        if (t < 0) {
+          // no more tiles: complete the next stage's phase without data so the
+          // MMA warp reads the end mark
+          const int s = (int)(kb % NST);
+          if (kb >= NST && !mbar_wait(&empty[s], (uint32_t)(((kb / NST) - 1) & 1), args.st, lim, 415)) break;
+          mbar_arrive(&full[s]);
+          break;
+        }
         int tm, tn;
         grouped_tile(t, ntm, ntn, 16, tm, tn);
         for (int kt = 0; kt < KT; kt++, kb++) {
@@ -335,9 +354,8 @@ gemm_lowp_persistent_kernel(const __grid_constant__ CUtensorMap mapA, const __gr
   } else if (warp == 1) {
     if (lane == 0) {  // ---- MMA issuer
       long long kb = 0;
-      int i = 0;
       bool ok = true;
-      for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, i++) {
+      for (int i = 0; ok; i++) {
         const int ab = i & 1, u = i >> 1;
         if (u >= 1 && !mbar_wait(&tempty[ab], (uint32_t)((u - 1) & 1), args.st, lim, 412)) break;
         tc_fence_after();
@@ -345,6 +363,11 @@ gemm_lowp_persistent_kernel(const __grid_constant__ CUtensorMap mapA, const __gr
         for (int kt = 0; kt < KT; kt++, kb++) {
           const int s = (int)(kb % NST);
           if (!mbar_wait(&full[s], (uint32_t)((kb / NST) & 1), args.st, lim, 413)) {
+            ok = false;
+            break;
+          }
+          if (kt == 0 && s_tiles[i & 7] < 0) {  // end mark: pass it on to the epilogue
+            mbar_arrive(&tfull[ab]);
             ok = false;
             break;
           }
@@ -371,7 +394,7 @@ gemm_lowp_persistent_kernel(const __grid_constant__ CUtensorMap mapA, const __gr
           }
           umma_commit(&empty[s]);
         }
-        umma_commit(&tfull[ab]);
+        if (ok) umma_commit(&tfull[ab]);
       }
     }
   } else {
@@ -382,15 +405,16 @@ gemm_lowp_persistent_kernel(const __grid_constant__ CUtensorMap mapA, const __gr
     // operands were scaled by powers of two; undo exactly on the accumulator
     const float unscale = args.amax ? pow2_unscale(args.amax) : 1.f;
     long long chunk = 0;
-    int i = 0;
-    for (int t = blockIdx.x; t < tiles; t += gridDim.x, i++) {
-      int tm, tn;
-      grouped_tile(t, ntm, ntn, 16, tm, tn);
+    for (int i = 0;; i++) {
       const int ab = i & 1, u = i >> 1;
       if (!mbar_wait(&tfull[ab], (uint32_t)(u & 1), args.st, lim, 414) && lane == 0) atomicOr(&s_epi_fail, 1);
       // agree across the four warps before the warp-collective loads
       epi_bar();
       const bool ok = *(volatile int*)&s_epi_fail == 0;
+      const int t = s_tiles[i & 7];
+      if (!ok || t < 0) break;
+      int tm, tn;
+      grouped_tile(t, ntm, ntn, 16, tm, tn);
       tc_fence_after();
       for (int c = 0; c < BN / EPI_COLS; c++, chunk++) {
         uint32_t v[32];
@@ -444,15 +468,18 @@ int gemm_bf16_init() {
 
 // Persistent launch: grid = min(tiles, max_ctas).  kpart > 0 selects the
 // pairs layout: operand rows [hi (kpart) | lo (kpart)], K = kpart, a
-// multiple of the 64-wide k block.
+// multiple of the 64-wide k block.  tile_ctr (zeroed before the first of
+// the launches that share it) hands out tiles dynamically, so several
+// launches of the same product, on different streams, split its tiles
+// between them; null: each CTA strides over the tiles.
 int launch_gemm_lowp_persistent(const CUtensorMap& mapA, const CUtensorMap& mapB, const CUtensorMap& mapC,
                                 int a_row0, int b_row0, int c_row0, int c_col0, int M, int N, int K, bool bf16,
                                 const unsigned* amax, DevStatus* st, long long spin, int max_ctas, cudaStream_t s,
-                                int kpart) {
+                                int kpart, unsigned* tile_ctr) {
   if (M <= 0 || N <= 0 || K <= 0) return LU_OK;
   if (c_col0 & 3) return LU_ERR_ALIGN;
   if (kpart > 0 && (kpart != K || (kpart % BK) || bf16)) return LU_ERR_ARG;
-  Bf16GemmArgs a{a_row0, b_row0, c_row0, c_col0, M, N, K, make_idesc(bf16), amax, st, spin, kpart};
+  Bf16GemmArgs a{a_row0, b_row0, c_row0, c_col0, M, N, K, make_idesc(bf16), amax, st, spin, kpart, tile_ctr};
   const int64_t tiles = (int64_t)ceil_div(N, BN) * ceil_div(M, BM);
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, std::max(1, max_ctas)));
   if (kpart > 0)
@@ -471,7 +498,7 @@ int launch_gemm_bf16_tc(const CUtensorMap& mapA, const CUtensorMap& mapB, const 
                         DevStatus* st, long long spin, cudaStream_t s) {
   if (M <= 0 || N <= 0 || K <= 0) return LU_OK;
   if (c_col0 & 3) return LU_ERR_ALIGN;  // TMA x coordinate * 4 bytes must be a multiple of 16
-  Bf16GemmArgs a{a_row0, b_row0, c_row0, c_col0, M, N, K, make_idesc(bf16), amax, st, spin};
+  Bf16GemmArgs a{a_row0, b_row0, c_row0, c_col0, M, N, K, make_idesc(bf16), amax, st, spin, 0, nullptr};
   const int64_t tiles = (int64_t)ceil_div(N, BN) * ceil_div(M, BM);
   if (tiles > INT32_MAX) return LU_ERR_UNSUPPORTED;
   gemm_bf16_tc_kernel<<<(unsigned)tiles, THREADS, SMEM_BYTES, s>>>(mapA, mapB, mapC, a);
@@ -496,12 +523,14 @@ extern "C" __attribute__((visibility("default"))) int lub_test_gemm_lowp(const f
   cudaStream_t s = (cudaStream_t)stream;
   // mode bits 0-7: 0 bf16, 1 scaled fp16, 2 split fp16 x3 (concatenated
   // parts), 3 split fp16 x3 in the pairs layout (persistent kernel only);
-  // bits 8+: CTA count of the persistent kernel (0: one CTA per tile)
-  const int pctas = mode >> 8;
+  // bits 8-15: CTA count of the persistent kernel (0: one CTA per tile);
+  // bits 16-23: CTA count of a second persistent launch on another stream,
+  // the two sharing a tile counter (dynamic tiles)
+  const int pctas = (mode >> 8) & 0xff, hctas = (mode >> 16) & 0xff;
   mode &= 0xff;
   if (M <= 0 || N <= 0 || K <= 0 || mode < 0 || mode > 3 || (ldc & 3) || (reinterpret_cast<uintptr_t>(C) & 15))
     return LU_ERR_ARG;
-  if (mode == 3 && pctas <= 0) return LU_ERR_ARG;
+  if ((mode == 3 || hctas > 0) && pctas <= 0) return LU_ERR_ARG;
   LUB_TRY(gemm_bf16_init());
   const bool pairs = mode == 3;
   const int nparts = mode == 2 ? 3 : (pairs ? 2 : 1);
@@ -513,9 +542,10 @@ extern "C" __attribute__((visibility("default"))) int lub_test_gemm_lowp(const f
   LUB_CUDA(cudaMalloc(&Lb, sizeof(__nv_bfloat16) * M * ldk));
   LUB_CUDA(cudaMalloc(&Ub, sizeof(__nv_bfloat16) * N * ldk));
   DevStatus* st = nullptr;
-  LUB_CUDA(cudaMalloc(&st, sizeof(DevStatus) + 16));
+  LUB_CUDA(cudaMalloc(&st, sizeof(DevStatus) + 32));
   unsigned* amax = reinterpret_cast<unsigned*>(st + 1);
-  LUB_CUDA(cudaMemsetAsync(st, 0, sizeof(DevStatus), s));
+  unsigned* ctr = amax + 4;
+  LUB_CUDA(cudaMemsetAsync(st, 0, sizeof(DevStatus) + 32, s));
   int rc = LU_OK;
   const bool bf16 = mode == 0;
   if (bf16) {
@@ -537,7 +567,26 @@ extern "C" __attribute__((visibility("default"))) int lub_test_gemm_lowp(const f
   if (rc == LU_OK) rc = encode_tmap_2d(&mU, dt, 2, Ub, Ke, N, ldk * 2, 64, 256, CU_TENSOR_MAP_SWIZZLE_128B);
   if (rc == LU_OK)
     rc = encode_tmap_2d(&mC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, N, M, ldc * 4, 32, 128, CU_TENSOR_MAP_SWIZZLE_128B);
-  if (rc == LU_OK && pctas > 0)
+  if (rc == LU_OK && hctas > 0) {
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    LUB_CUDA(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+    LUB_CUDA(cudaEventCreateWithFlags(&e0, cudaEventDisableTiming));
+    LUB_CUDA(cudaEventCreateWithFlags(&e1, cudaEventDisableTiming));
+    LUB_CUDA(cudaEventRecord(e0, s));
+    LUB_CUDA(cudaStreamWaitEvent(s2, e0, 0));
+    rc = launch_gemm_lowp_persistent(mL, mU, mC, 0, 0, 0, 0, M, N, Kg, bf16, bf16 ? nullptr : amax, st, 1LL << 24,
+                                     pctas, s, pairs ? kps : 0, ctr);
+    if (rc == LU_OK)
+      rc = launch_gemm_lowp_persistent(mL, mU, mC, 0, 0, 0, 0, M, N, Kg, bf16, bf16 ? nullptr : amax, st,
+                                       1LL << 24, hctas, s2, pairs ? kps : 0, ctr);
+    LUB_CUDA(cudaEventRecord(e1, s2));
+    LUB_CUDA(cudaStreamWaitEvent(s, e1, 0));
+    LUB_CUDA(cudaStreamSynchronize(s));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s2);
+  } else if (rc == LU_OK && pctas > 0)
     rc = launch_gemm_lowp_persistent(mL, mU, mC, 0, 0, 0, 0, M, N, Kg, bf16, bf16 ? nullptr : amax, st, 1LL << 24,
                                      pctas, s, pairs ? kps : 0);
   else if (rc == LU_OK)

@@ -56,6 +56,7 @@ struct lu_handle_s {
   // (B200, N = 65536, FP16x3 with look-ahead: 48 SMs reserved and a 48-CTA
   // leaf measured best)
   int gemm_ctas = 148, gemm_reserve = 48;
+  int gemm_helper = 1;  // look-ahead: reserved SMs join the update once the panel is done
   int32_t* perm = nullptr;
   int32_t* perm_work = nullptr;
   int32_t* perm_lists = nullptr;  // composed pivot batches (ipiv -> perm)

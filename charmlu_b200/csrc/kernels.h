@@ -135,11 +135,12 @@ int launch_gemm_bf16_tc(const CUtensorMap& mapA, const CUtensorMap& mapB, const 
                         DevStatus* st, long long spin, cudaStream_t s);
 // persistent variant: max_ctas CTAs walk the tiles (TMEM double-buffered);
 // kpart > 0: error-compensated pairs layout [hi | lo] per operand row, the
-// three products Lh*Uh + Lh*Ul + Ll*Uh from one stage, K = kpart
+// three products Lh*Uh + Lh*Ul + Ll*Uh from one stage, K = kpart;
+// tile_ctr: a zeroed counter shared by launches that split the tiles
 int launch_gemm_lowp_persistent(const CUtensorMap& mapA, const CUtensorMap& mapB, const CUtensorMap& mapC,
                                 int a_row0, int b_row0, int c_row0, int c_col0, int M, int N, int K, bool bf16,
                                 const unsigned* amax, DevStatus* st, long long spin, int max_ctas, cudaStream_t s,
-                                int kpart = 0);
+                                int kpart = 0, unsigned* tile_ctr = nullptr);
 // |max| of the L21 (rows x K) and U12 (K x N) FP32 panels into amax[0], amax[1]
 int launch_panel_absmax(const float* L, int64_t ldl, int rows, int K, const float* U, int64_t ldu, int N,
                         unsigned* amax, cudaStream_t s);

@@ -282,7 +282,9 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
   h->spin = cfg->spin_limit > 0 ? cfg->spin_limit : (1LL << 24);
   const int64_t n = cfg->n;
   int s = LU_OK;
-  h->n_counters = (int)(n / 2 + 1024);  // one per leaf launch; leaves are >= 2 columns wide
+  // one per leaf launch (leaves are >= 2 columns wide) and one per shared
+  // trailing-update tile counter (panels are >= 64 columns wide)
+  h->n_counters = (int)(n / 2 + n / 64 + 1024);
   if (s == LU_OK) s = h->alloc(&h->st, 1);
   if (s == LU_OK) s = h->alloc(&h->counters, h->n_counters);
   if (s == LU_OK) s = h->alloc(&h->leaf64.cand_val, 2 * kMaxLeafCTAs);
@@ -321,6 +323,7 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
   if (const char* e = getenv("LU_B200_LEAF_W32_LA")) h->leaf_w32_la = std::min(64, std::max(4, atoi(e)));
   if (const char* e = getenv("LU_B200_GEMM_CTAS")) h->gemm_ctas = std::max(0, atoi(e));
   if (const char* e = getenv("LU_B200_GEMM_RESERVE")) h->gemm_reserve = std::max(0, atoi(e));
+  if (const char* e = getenv("LU_B200_GEMM_HELPER")) h->gemm_helper = atoi(e) != 0;
   if (const char* e = getenv("LU_B200_STAGE_BYTES")) h->stage_bytes = std::max<size_t>(1 << 16, strtoull(e, nullptr, 10));
   if (const char* e = getenv("LU_B200_RESIDENT_BYTES")) h->resident_cap = strtoull(e, nullptr, 10);
   if (s == LU_OK) s = h->alloc(&h->perm, n);

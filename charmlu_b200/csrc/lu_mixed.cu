@@ -160,14 +160,21 @@ int build_operands(lu_handle h, const Ctx32& c, int k0, int kw, int k1, int rest
 // (reserve: SMs left free for a panel running beside it).  K and kpart as
 // from build_operands; flops are counted as executed on the panel's kw
 // columns (three products for the FP16 split).
+// tile_ctr: a zeroed counter shared with a helper launch of the same
+// product (helper_ctas > 0 makes this call that helper: it is not timed as
+// a phase, since the main launch's span covers the whole product).
 int lowp_gemm(lu_handle h, const CUtensorMap& mapL, const CUtensorMap& mapU, const CUtensorMap& mapC, int k1,
-              int rest, int u0, int ncols, int K, int kpart, int kw, bool bf16, cudaStream_t s, int reserve = 0) {
+              int rest, int u0, int ncols, int K, int kpart, int kw, bool bf16, cudaStream_t s, int reserve = 0,
+              unsigned* tile_ctr = nullptr, int helper_ctas = 0) {
+  const unsigned* amax = bf16 ? nullptr : h->amax;
+  if (helper_ctas > 0)
+    return launch_gemm_lowp_persistent(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, K, bf16, amax, h->st,
+                                       h->spin, helper_ctas, s, kpart, tile_ctr);
   const int prods = bf16 ? 1 : (h->cfg.precision == LU_PREC_FP16X3 ? 3 : 1);
   Prof pf(h, s, LU_PH_GEMM, 2.0 * rest * (double)ncols * kw * prods);
-  const unsigned* amax = bf16 ? nullptr : h->amax;
   if (h->gemm_ctas > 0)
     return launch_gemm_lowp_persistent(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, K, bf16, amax, h->st,
-                                       h->spin, std::max(1, h->gemm_ctas - reserve), s, kpart);
+                                       h->spin, std::max(1, h->gemm_ctas - reserve), s, kpart, tile_ctr);
   return launch_gemm_bf16_tc(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, K, bf16, amax, h->st, h->spin, s);
 }
 
@@ -221,9 +228,18 @@ int factor_mixed(lu_handle h, cudaStream_t s) {
     LUB_CUDA(cudaEventRecord(h->evN, s));
     LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evN, 0));
     LUB_TRY(panel32(cp, k1, nw, k1, nw));
+    // The rest of update k runs on the SMs the panel leaves free; once the
+    // panel is done, a helper launch on its stream takes the remaining
+    // tiles from the same counter, so the reserved SMs do not idle.
+    unsigned* ctr =
+        (rest > nw && h->gemm_helper && h->gemm_ctas > 0 && h->gemm_reserve > 0) ? h->take_counter() : nullptr;
+    if (ctr)
+      LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, nw, rest - nw, K, kpart, kw, bf16, h->sP, 0, ctr,
+                        h->gemm_reserve));
     LUB_CUDA(cudaEventRecord(h->evP, h->sP));
     if (rest > nw)
-      LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, nw, rest - nw, K, kpart, kw, bf16, s, h->gemm_reserve));
+      LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, nw, rest - nw, K, kpart, kw, bf16, s, h->gemm_reserve,
+                        ctr));
   }
   return LU_OK;
 }

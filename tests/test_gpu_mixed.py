@@ -101,6 +101,29 @@ def test_gemm_lowp_persistent_matches_tile_kernel(cuda_dev, M, N, K, mode, pctas
     assert torch.equal(C0, C1)
 
 
+@pytest.mark.parametrize("mode", [0, 2, 3])
+@pytest.mark.parametrize("pctas,hctas", [(100, 48), (1, 1), (3, 5), (116, 32)])
+@pytest.mark.parametrize("M,N,K", [(300, 520, 256), (1100, 2100, 192), (4096, 4096, 256)])
+def test_gemm_lowp_shared_tile_counter(cuda_dev, M, N, K, mode, pctas, hctas):
+    """Two persistent launches on two streams that take tiles from one
+    counter (the look-ahead update and its helper) give the same C bit for
+    bit as one launch: each tile is computed once, by whichever CTA takes it."""
+    f = _lib()
+    g = torch.Generator(device="cuda").manual_seed(M + 5 * N + pctas + hctas)
+    A = torch.rand(M, K, device="cuda", generator=g, dtype=torch.float32) - 0.5
+    B = (torch.rand(K, N, device="cuda", generator=g, dtype=torch.float32) - 0.5) * 5.0
+    ldc = (N + 3) // 4 * 4
+    C0 = torch.rand(M, ldc, device="cuda", generator=g, dtype=torch.float32) - 0.5
+    C1 = C0.clone()
+    st = torch.cuda.current_stream().cuda_stream
+    single = mode | ((148 << 8) if mode == 3 else 0)
+    assert f(A.data_ptr(), K, B.data_ptr(), N, C0.data_ptr(), ldc, M, N, K, single, st) == 0
+    assert f(A.data_ptr(), K, B.data_ptr(), N, C1.data_ptr(), ldc, M, N, K, mode | (pctas << 8) | (hctas << 16),
+             st) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(C0, C1)
+
+
 def _refine(n, b, A_np=None, seed=42, mode=None, target=16.0, prec=None, lookahead=False):
     import charmlu_b200 as lu
     prec = lu.LU_PREC_FP16X3 if prec is None else prec
@@ -201,6 +224,24 @@ def test_kappa_matrices_refine_or_report(cuda_dev, kappa):
         s = lu.LUSolver(lu.LUConfig(n, 256, precision=lu.LU_PREC_FP16X3))
         x, info = s.refine_solve(A, b)
         assert s.status() == 0 and info["used_gmres"] == 0
+
+
+@pytest.mark.parametrize("n,b", [(4096, 512), (3000, 192)])
+def test_refine_update_helper_bitwise(cuda_dev, n, b, monkeypatch):
+    """Under look-ahead the reserved SMs join the trailing update once the
+    panel is done (a helper launch sharing the update's tile counter). The
+    factors, and so x, are the same bit for bit as without the helper."""
+    import charmlu_b200 as lu
+    A = lu.generate_uniform(n, n, seed=5, stream_id=0)
+    rhs = lu.generate_uniform(n, 1, seed=5, stream_id=1).view(-1)
+    xs = []
+    for helper in ("1", "0"):
+        monkeypatch.setenv("LU_B200_GEMM_HELPER", helper)
+        s = lu.LUSolver(lu.LUConfig(n, b, precision=lu.LU_PREC_FP16X3, lookahead=True))
+        x, info = s.refine_solve(A, rhs)
+        assert s.status() == 0 and info["status"] == 0, info
+        xs.append(x)
+    assert torch.equal(xs[0], xs[1])
 
 
 def test_refine_graph_replay(cuda_dev):
