@@ -2,6 +2,7 @@
 // shared by the FP64 and mixed-precision orchestration.
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <algorithm>
 #include <vector>
 
@@ -57,6 +58,14 @@ struct lu_handle_s {
   // leaf measured best)
   int gemm_ctas = 148, gemm_reserve = 48;
   int gemm_helper = 1;  // look-ahead: reserved SMs join the update once the panel is done
+  // FP16x3 mixed path: the recursive FP32 panel's GEMM halves of width >= 128
+  // on the tcgen05 kernel, with their own split-operand buffers (the panel
+  // runs beside the trailing update, which owns Lb/Ub/amax)
+  int panel_tc = 0;
+  __half* Lp = nullptr;
+  __half* Up = nullptr;
+  unsigned* amaxP = nullptr;
+  int64_t ldkP = 0;
   int32_t* perm = nullptr;
   int32_t* perm_work = nullptr;
   int32_t* perm_lists = nullptr;  // composed pivot batches (ipiv -> perm)

@@ -324,6 +324,7 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
   if (const char* e = getenv("LU_B200_GEMM_CTAS")) h->gemm_ctas = std::max(0, atoi(e));
   if (const char* e = getenv("LU_B200_GEMM_RESERVE")) h->gemm_reserve = std::max(0, atoi(e));
   if (const char* e = getenv("LU_B200_GEMM_HELPER")) h->gemm_helper = atoi(e) != 0;
+  if (const char* e = getenv("LU_B200_PANEL_TC")) h->panel_tc = atoi(e) != 0;
   if (const char* e = getenv("LU_B200_STAGE_BYTES")) h->stage_bytes = std::max<size_t>(1 << 16, strtoull(e, nullptr, 10));
   if (const char* e = getenv("LU_B200_RESIDENT_BYTES")) h->resident_cap = strtoull(e, nullptr, 10);
   if (s == LU_OK) s = h->alloc(&h->perm, n);

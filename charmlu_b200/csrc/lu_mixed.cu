@@ -40,6 +40,12 @@ int ensure_mixed(lu_handle h) {
   LUB_TRY(h->alloc(&h->Ub, (size_t)n * h->ldk));
   LUB_TRY(h->alloc(&h->ipiv32, n));
   LUB_TRY(h->alloc(&h->amax, 4));
+  if (h->pairs && h->panel_tc) {  // panel GEMM operands: K <= B/2 rows of [hi | lo], N <= B/2 columns
+    h->ldkP = 2 * ((B / 2 + 63) & ~int64_t(63));
+    LUB_TRY(h->alloc(&h->Lp, (size_t)n * h->ldkP));
+    LUB_TRY(h->alloc(&h->Up, (size_t)B * h->ldkP));
+    LUB_TRY(h->alloc(&h->amaxP, 4));
+  }
   LUB_TRY(h->alloc(&h->v32, n));
   LUB_TRY(h->alloc(&h->r64, n));
   LUB_TRY(h->alloc(&h->z64, n));
@@ -98,6 +104,31 @@ int trsm32(Ctx32& c, int r0, int w, int rb, int cb, int ncols) {
   return trsm32(c, r0 + w1, w - w1, rb + w1, cb, ncols);
 }
 
+// C(r0.., n0..n0+N) -= L(r0.., kc..kc+K) * U(kc..kc+K, n0..n0+N) inside the
+// panel that ends at column cend, on the tcgen05 kernel: both operands split
+// into scaled FP16 hi/lo parts (pairs layout, three products), as the
+// trailing update does. The C tensor map ends at cend, so the 256-wide tiles
+// leave the columns right of the panel (being updated beside it) untouched.
+int panel_gemm_tc(Ctx32& c, int r0, int M, int kc, int K, int n0, int N, int cend) {
+  lu_handle h = c.h;
+  Prof pf(h, c.s, LU_PH_GEMM_IN, 2.0 * M * (double)N * K);
+  const float* L = c.A + (int64_t)r0 * c.ld + kc;
+  const float* U = c.A + (int64_t)kc * c.ld + n0;
+  LUB_TRY(launch_panel_absmax(L, c.ld, M, K, U, c.ld, N, h->amaxP, c.s));
+  LUB_TRY(launch_split_rows<__half>(L, c.ld, h->Lp, h->ldkP, M, K, 2, 0x2u, h->amaxP, 0, c.s, K));
+  LUB_TRY(launch_split_transpose<__half>(U, c.ld, h->Up, h->ldkP, K, N, 2, 0x2u, h->amaxP, 1, c.s, K));
+  CUtensorMap mL, mU, mC;
+  LUB_TRY(encode_tmap_2d(&mL, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, h->Lp, 2 * K, M, h->ldkP * 2, 64, 128,
+                         CU_TENSOR_MAP_SWIZZLE_128B));
+  LUB_TRY(encode_tmap_2d(&mU, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, h->Up, 2 * K, N, h->ldkP * 2, 64, 256,
+                         CU_TENSOR_MAP_SWIZZLE_128B));
+  LUB_TRY(encode_tmap_2d(&mC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, c.A, cend, c.n, c.ld * 4, 32, 128,
+                         CU_TENSOR_MAP_SWIZZLE_128B));
+  const int ctas = h->cfg.lookahead ? h->gemm_reserve : h->gemm_ctas;
+  return launch_gemm_lowp_persistent(mL, mU, mC, 0, 0, r0, n0, M, N, K, false, h->amaxP, h->st, h->spin,
+                                     std::max(1, ctas), c.s, K);
+}
+
 // recursive FP32 panel of columns [c0, c0+w) inside the panel [p0, p0+pw);
 // the leaves swap rows across the whole panel (no laswp in the recursion)
 int panel32(Ctx32& c, int c0, int w, int p0, int pw) {
@@ -113,7 +144,11 @@ int panel32(Ctx32& c, int c0, int w, int p0, int pw) {
   const int w1 = split_w32(w), w2 = w - w1;
   LUB_TRY(panel32(c, c0, w1, p0, pw));
   LUB_TRY(trsm32(c, c0, w1, c0, c0 + w1, w2));
-  LUB_TRY(sgemm(c, c0 + w1, c0 + w1, c0 + w1, c0, c0, c0 + w1, M - w1, w2, w1));
+  if (c.h->Lp && w2 >= 128 && w1 % 64 == 0 && 2 * w1 <= c.h->ldkP && w2 <= c.h->cfg.block_size &&
+      (c0 + w1) % 4 == 0)
+    LUB_TRY(panel_gemm_tc(c, c0 + w1, M - w1, c0, w1, c0 + w1, w2, p0 + pw));
+  else
+    LUB_TRY(sgemm(c, c0 + w1, c0 + w1, c0 + w1, c0, c0, c0 + w1, M - w1, w2, w1));
   return panel32(c, c0 + w1, w2, p0, pw);
 }
 

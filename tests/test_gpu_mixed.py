@@ -244,6 +244,30 @@ def test_refine_update_helper_bitwise(cuda_dev, n, b, monkeypatch):
     assert torch.equal(xs[0], xs[1])
 
 
+@pytest.mark.parametrize("n,b,la", [(4096, 512, True), (3000, 256, True), (2048, 512, False), (1500, 192, True)])
+def test_refine_panel_gemm_tensor_cores(cuda_dev, n, b, la, monkeypatch):
+    """LU_B200_PANEL_TC=1 moves the recursive panel's GEMM halves (width >=
+    128) onto the tcgen05 kernel with split FP16 operands. Refinement reaches
+    the target as quickly, and x agrees with the FP32-SIMT panel's x to the
+    accuracy the HPL bar leaves (forward error ~ kappa * n * eps * 16)."""
+    import charmlu_b200 as lu
+    A = lu.generate_uniform(n, n, seed=9, stream_id=0)
+    rhs = lu.generate_uniform(n, 1, seed=9, stream_id=1).view(-1)
+    out = []
+    for tc in ("0", "1"):
+        monkeypatch.setenv("LU_B200_PANEL_TC", tc)
+        s = lu.LUSolver(lu.LUConfig(n, b, precision=lu.LU_PREC_FP16X3, lookahead=la))
+        x, info = s.refine_solve(A, rhs)
+        assert s.status() == 0 and info["status"] == 0, info
+        assert info["used_gmres"] == 0 and info["iterations"] <= 4, info
+        assert s.residual(A, x, rhs)["r_hpl"] < 16
+        out.append(x)
+    x_ref, *_ = oracle.solve(A.cpu().numpy(), rhs.cpu().numpy(), b=128)
+    for x in out:
+        fe = np.abs(x.cpu().numpy() - x_ref).max() / np.abs(x_ref).max()
+        assert fe < 1e-6, fe
+
+
 def test_refine_graph_replay(cuda_dev):
     import charmlu_b200 as lu
     n, b = 2048, 256
