@@ -22,7 +22,8 @@ EXPORTS = [
     "lu_batched_factor_solve", "lu_generate_uniform", "lu_matgen_host", "lu_status_string",
     "lu_profile", "lu_phase_times", "lu_launch_count", "lu_solve_noalloc",
     "lu_batched_work_bytes", "lu_batched_set_tuning", "lu_refine_factor", "lu_refine_apply",
-    "lu_refine_adjoint",
+    "lu_refine_adjoint", "lu_panel_factor", "lu_apply_pivots", "lu_trsm_lower_unit", "lu_gemm_update",
+    "lu_trsv_block", "lu_gemv_update",
 ]
 PHASES = ["panel", "laswp", "trsm", "gemm", "gemm_inner", "solve", "other"]
 
@@ -71,6 +72,12 @@ def load():
         "lu_residual": ([H, P, i64, P, P, ctypes.POINTER(LuResidualInfo), P], ctypes.c_int),
         "lu_refine_solve": ([H, P, i64, P, P, ctypes.POINTER(LuRefineInfo), P], ctypes.c_int),
         "lu_refine_solve_host": ([H, P, i64, P, P, ctypes.POINTER(LuRefineInfo), P], ctypes.c_int),
+        "lu_panel_factor": ([H, P, i64, i64, i32, P, i64, P], ctypes.c_int),
+        "lu_apply_pivots": ([H, P, i64, i32, P, i64, i32, i32, i32, P, P], ctypes.c_int),
+        "lu_trsm_lower_unit": ([H, P, i64, i32, P, i64, i64, P], ctypes.c_int),
+        "lu_gemm_update": ([H, P, i64, P, i64, P, i64, i64, i64, i64, P], ctypes.c_int),
+        "lu_trsv_block": ([H, P, i64, i32, i32, P, P], ctypes.c_int),
+        "lu_gemv_update": ([H, P, i64, i64, i32, P, P, P], ctypes.c_int),
         "lu_adjoint": ([H, P, i64, P, P, i64, P, i64, i64, P, i64, P, i64, P], ctypes.c_int),
         "lu_refine_factor": ([H, P, i64, P], ctypes.c_int),
         "lu_refine_apply": ([H, P, i64, i32, P, i64, P, i64, i64, ctypes.POINTER(LuRefineInfo), P], ctypes.c_int),

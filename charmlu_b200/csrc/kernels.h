@@ -110,6 +110,8 @@ struct ResidualAccum {  // non-negative doubles stored as ordered bit patterns
 };
 int launch_residual_f64(const double* A, int64_t lda, int n, const double* x, const double* b, double* r,
                         ResidualAccum* acc, cudaStream_t s);
+// y[0:m] -= A[0:m, 0:k] x (one warp per row)
+int launch_gemv_sub(const double* A, int64_t lda, int m, int k, const double* x, double* y, cudaStream_t s);
 // the same for rows row0 .. row0 + rows - 1 only (Arows = their first row);
 // accumulates into acc without clearing it
 int launch_residual_f64_rows(const double* Arows, int64_t lda, int rows, int row0, int n, const double* x,

@@ -96,6 +96,7 @@ struct Ctx64 {
   PivotList pl;
   int leaf_w;
   int leaf_ctas;
+  int base = 0;  // global row/column of the matrix's first row (a panel view)
 };
 
 int pivots_apply_f64(Ctx64& c, int k0, int cnt, int c_begin, int c_end, int skip_b, int skip_e, double* rhs,
@@ -142,8 +143,9 @@ int panel64(Ctx64& c, int c0, int w, int p0, int pw) {
     unsigned* bar = c.h->take_counter();
     if (!bar) return LU_ERR_NOMEM;
     Prof pf(c.h, c.s, LU_PH_PANEL, (double)M * w * w);
-    return launch_getf2_leaf<double>(c.A.at(c0, c0), c.A.ld, M, w, c.ipiv + c0, c0, c.h->leaf64, bar, c.h->st, c0,
-                                     c.thr, c.h->spin, c.leaf_ctas, c.s, c.A.at(c0, p0), pw, c0 - p0);
+    return launch_getf2_leaf<double>(c.A.at(c0, c0), c.A.ld, M, w, c.ipiv + c0, c.base + c0, c.h->leaf64, bar,
+                                     c.h->st, c.base + c0, c.thr, c.h->spin, c.leaf_ctas, c.s, c.A.at(c0, p0), pw,
+                                     c0 - p0);
   }
   const int w1 = split_w(w), w2 = w - w1;
   LUB_TRY(panel64(c, c0, w1, p0, pw));
@@ -554,6 +556,126 @@ const char* lu_status_string(int status) {
     case LU_ERR_UNSUPPORTED: return "unsupported configuration";
     default: return "unknown status";
   }
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Per-block building blocks for callers that distribute the matrix
+// themselves (the block-cyclic multi-GPU driver): the same recursion and
+// kernels as lu_factor / lu_solve, on caller-supplied views.
+// ---------------------------------------------------------------------------
+namespace {
+
+int check_view(const void* p, int64_t ld, int64_t cols) {
+  if (!p || ld <= 0 || ld < cols) return LU_ERR_ARG;
+  if ((ld & 1) || (reinterpret_cast<uintptr_t>(p) & 15)) return LU_ERR_ALIGN;
+  return LU_OK;
+}
+
+Ctx64 block_ctx(lu_handle h, cudaStream_t s) {
+  const bool la = h->cfg.lookahead != 0;
+  Ctx64 c;
+  c.h = h;
+  c.ipiv = nullptr;
+  c.n = 0;
+  c.s = s;
+  c.thr = h->cfg.sing_threshold;
+  c.pl = h->plist;
+  c.leaf_w = la ? h->leaf_w64_la : h->leaf_w64;
+  c.leaf_ctas = la ? h->leaf_ctas_la : h->leaf_ctas;
+  return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lu_panel_factor(lu_handle h, double* dP, int64_t ldp, int64_t m, int32_t w, int32_t* d_ipiv, int64_t base,
+                    void* stream) {
+  if (!h || !d_ipiv || w < 1 || m < w || m > h->cfg.n || base < 0 || base + m > ((int64_t)1 << 31) - 1)
+    return LU_ERR_ARG;
+  LUB_TRY(check_view(dP, ldp, w));
+  LUB_TRY(ensure_kernels_init());
+  cudaStream_t s = (cudaStream_t)stream;
+  Ctx64 c = block_ctx(h, s);
+  c.ipiv = d_ipiv;
+  c.n = (int)m;
+  c.base = (int)base;
+  LUB_TRY(c.A.init(dP, m, w, ldp));
+  // one barrier counter per leaf, from a pool cleared for this panel
+  LUB_CUDA(cudaMemsetAsync(h->counters, 0, sizeof(unsigned) * h->n_counters, s));
+  h->next_counter = 0;
+  return panel64(c, 0, w, 0, w);
+}
+
+int lu_apply_pivots(lu_handle h, double* dA, int64_t lda, int32_t ncols, const int32_t* d_ipiv, int64_t k0,
+                    int32_t cnt, int32_t skip_b, int32_t skip_e, double* db, void* stream) {
+  if (!h || !d_ipiv || ncols < 0 || cnt < 0 || k0 < 0 || k0 + cnt > ((int64_t)1 << 31) - 1) return LU_ERR_ARG;
+  if (ncols > 0) LUB_TRY(check_view(dA, lda, ncols));
+  LUB_TRY(ensure_kernels_init());
+  cudaStream_t s = (cudaStream_t)stream;
+  Prof pf(h, s, LU_PH_LASWP);
+  for (int off = 0; off < cnt; off += 512) {
+    const int sub = std::min(512, cnt - off);
+    LUB_TRY(launch_pivot_compose(d_ipiv, (int)k0 + off, sub, h->plist, s));
+    LUB_TRY(launch_pivot_apply<double>(dA, lda, 0, ncols, skip_b, skip_e, h->plist, 2 * sub, db, nullptr, s));
+  }
+  return LU_OK;
+}
+
+int lu_trsm_lower_unit(lu_handle h, const double* dL, int64_t ldl, int32_t w, double* dB, int64_t ldb, int64_t ncols,
+                       void* stream) {
+  if (!h || w < 1 || ncols < 0 || ncols > ((int64_t)1 << 31) - 1) return LU_ERR_ARG;
+  if (ncols == 0) return LU_OK;
+  LUB_TRY(check_view(dL, ldl, w));
+  LUB_TRY(check_view(dB, ldb, ncols));
+  LUB_TRY(ensure_kernels_init());
+  Ctx64 c = block_ctx(h, (cudaStream_t)stream);
+  MatF64 Lm, Bm;
+  LUB_TRY(Lm.init(const_cast<double*>(dL), w, w, ldl));
+  LUB_TRY(Bm.init(dB, w, ncols, ldb));
+  return trsm64(c, Lm, 0, w, Bm, 0, 0, (int)ncols);
+}
+
+int lu_gemm_update(lu_handle h, const double* dA, int64_t lda, const double* dB, int64_t ldb, double* dC, int64_t ldc,
+                   int64_t M, int64_t N, int64_t K, void* stream) {
+  const int64_t lim = ((int64_t)1 << 31) - 1;
+  if (!h || M < 0 || N < 0 || K < 0 || M > lim || N > lim || K > lim) return LU_ERR_ARG;
+  if (M == 0 || N == 0 || K == 0) return LU_OK;
+  LUB_TRY(check_view(dA, lda, K));
+  LUB_TRY(check_view(dB, ldb, N));
+  LUB_TRY(check_view(dC, ldc, N));
+  LUB_TRY(ensure_kernels_init());
+  Ctx64 c = block_ctx(h, (cudaStream_t)stream);
+  MatF64 Am, Bm, Cm;
+  LUB_TRY(Am.init(const_cast<double*>(dA), M, K, lda));
+  LUB_TRY(Bm.init(const_cast<double*>(dB), K, N, ldb));
+  Cm.p = dC;
+  Cm.ld = ldc;
+  Cm.rows = M;
+  Cm.cols = N;
+  return gemm64(c, Cm, 0, 0, Am, 0, 0, Bm, 0, 0, (int)M, (int)N, (int)K, LU_PH_GEMM);
+}
+
+int lu_trsv_block(lu_handle h, const double* dT, int64_t ldt, int32_t w, int32_t upper, double* dx, void* stream) {
+  if (!h || !dx || w < 1 || w > h->cfg.n) return LU_ERR_ARG;
+  LUB_TRY(check_view(dT, ldt, w));
+  LUB_TRY(ensure_kernels_init());
+  cudaStream_t s = (cudaStream_t)stream;
+  Prof pf(h, s, LU_PH_SOLVE, (double)w * w);
+  return launch_trsv<double>(dT, ldt, w, dx, upper ? 1 : 0, h->trsv_flags, h->trsv_ticket, h->st, h->spin, s);
+}
+
+int lu_gemv_update(lu_handle h, const double* dA, int64_t lda, int64_t m, int32_t k, const double* dx, double* dy,
+                   void* stream) {
+  if (!h || !dx || !dy || m < 0 || k < 0 || m > ((int64_t)1 << 31) - 1) return LU_ERR_ARG;
+  if (m == 0 || k == 0) return LU_OK;
+  LUB_TRY(check_view(dA, lda, k));
+  LUB_TRY(ensure_kernels_init());
+  cudaStream_t s = (cudaStream_t)stream;
+  Prof pf(h, s, LU_PH_SOLVE, 2.0 * (double)m * k);
+  return launch_gemv_sub(dA, lda, (int)m, k, dx, dy, s);
 }
 
 }  // extern "C"

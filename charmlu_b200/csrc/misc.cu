@@ -84,6 +84,34 @@ __global__ void __launch_bounds__(256) residual_f64_kernel(const double* A, int6
   }
 }
 
+// y[i] -= A[i, :] . x for i < m (one warp per row; k columns)
+__global__ void __launch_bounds__(256) gemv_sub_kernel(const double* A, int64_t lda, int m, int k, const double* x,
+                                                       double* y) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * 8 + warp;
+  if (row >= m) return;
+  const double* ar = A + (int64_t)row * lda;
+  double s0 = 0.0, s1 = 0.0;
+  const bool vec = ((lda & 1) == 0) && ((reinterpret_cast<uintptr_t>(A) & 15) == 0) &&
+                   ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
+  if (vec) {
+    const int k2 = k & ~1;
+    for (int j = lane * 2; j < k2; j += 64) {
+      const double2 a = *reinterpret_cast<const double2*>(ar + j);
+      const double2 xv = *reinterpret_cast<const double2*>(x + j);
+      s0 = fma(a.x, xv.x, s0);
+      s1 = fma(a.y, xv.y, s1);
+    }
+    if ((k & 1) && lane == 0) s0 = fma(ar[k - 1], x[k - 1], s0);
+  } else {
+    for (int j = lane; j < k; j += 32) s0 = fma(ar[j], x[j], s0);
+  }
+  double s = s0 + s1;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) y[row] -= s;
+}
+
 __global__ void gen_uniform_kernel(double* d, int64_t rows, int64_t cols, int64_t ld, uint64_t key) {
   const int64_t total = rows * cols;
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
@@ -113,6 +141,13 @@ int launch_residual_f64(const double* A, int64_t lda, int n, const double* x, co
   LUB_CUDA(cudaMemsetAsync(acc, 0, sizeof(ResidualAccum), s));
   if (n <= 0) return LU_OK;
   residual_f64_kernel<<<ceil_div(n, 8), 256, 0, s>>>(A, lda, n, 0, n, x, b, r, acc);
+  LUB_LAUNCH_CHECK();
+  return LU_OK;
+}
+
+int launch_gemv_sub(const double* A, int64_t lda, int m, int k, const double* x, double* y, cudaStream_t s) {
+  if (m <= 0 || k <= 0) return LU_OK;
+  gemv_sub_kernel<<<ceil_div(m, 8), 256, 0, s>>>(A, lda, m, k, x, y);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }

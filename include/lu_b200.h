@@ -271,6 +271,56 @@ LU_API int lu_matgen_host(double* out, int64_t count, int32_t seed, int64_t skip
 #define LU_NUM_PHASES 7
 LU_API int lu_profile(lu_handle h, int enable);
 LU_API int lu_phase_times(lu_handle h, double* ms, int64_t* launches, double* flops);
+/* ---- Per-block building blocks ------------------------------------------
+ * For callers that distribute the matrix themselves, such as the 1D
+ * block-cyclic multi-GPU driver (charmlu_b200/distributed.py), which keeps
+ * each GPU's column blocks and broadcasts panels over NCCL as the
+ * reference's block chares do with messages.  Each call uses the same
+ * kernels as lu_factor / lu_solve on caller-supplied views: FP64,
+ * row-major, even leading dimension, 16-byte aligned base, asynchronous on
+ * stream.  The handle supplies workspace; its order n bounds m and w. */
+
+/* LU with partial pivoting of the m x w panel dP (m >= w): the pivot search
+ * runs over all m rows and rows are swapped across the panel's w columns.
+ * d_ipiv[j] (device) = base + the 0-based panel row chosen for column j, so
+ * with base = the panel's first global row it holds global rows as in
+ * lu_factor.  A singular column is recorded for lu_status as base + j + 1.
+ * Replaces the panel phase of LUBlk::factor: pivot search and reduction,
+ * multipliers, rank-1 updates and in-panel swaps (lu.ci:256-370;
+ * lu.C:197-288, 166-177). */
+LU_API int lu_panel_factor(lu_handle h, double* dP, int64_t ldp, int64_t m, int32_t w, int32_t* d_ipiv,
+                           int64_t base, void* stream);
+
+/* Row interchanges d_ipiv[k0 .. k0+cnt) (device, global 0-based rows, in
+ * order) on columns [0, ncols) of dA, except the columns [skip_b, skip_e)
+ * that already hold them (the factored panel); db (optional, device) is
+ * permuted too.  dA must have every row the pivots name.  Replaces the
+ * pivot batches applied to the other block columns and to b
+ * (sendPendingPivots / applySwap, lu.C:46-169; pivotBatch, lu.ci:92-123). */
+LU_API int lu_apply_pivots(lu_handle h, double* dA, int64_t lda, int32_t ncols, const int32_t* d_ipiv, int64_t k0,
+                           int32_t cnt, int32_t skip_b, int32_t skip_e, double* db, void* stream);
+
+/* dB (w x ncols) <- L^{-1} dB with L the unit lower triangle of dL (w x w).
+ * Replaces LUBlk::computeU (lu.C:180-189). */
+LU_API int lu_trsm_lower_unit(lu_handle h, const double* dL, int64_t ldl, int32_t w, double* dB, int64_t ldb,
+                              int64_t ncols, void* stream);
+
+/* dC (M x N) -= dA (M x K) * dB (K x N) on the FP64 tensor cores.
+ * Replaces LUBlk::updateMatrix (lu.C:26-43). */
+LU_API int lu_gemm_update(lu_handle h, const double* dA, int64_t lda, const double* dB, int64_t ldb, double* dC,
+                          int64_t ldc, int64_t M, int64_t N, int64_t K, void* stream);
+
+/* dx (w) <- L^{-1} dx (upper = 0, unit lower) or U^{-1} dx (upper = 1) for
+ * one w x w diagonal block dT.  Replaces the diagonal solves of
+ * forwardSolve / backwardSolve (lu.ci:387-436). */
+LU_API int lu_trsv_block(lu_handle h, const double* dT, int64_t ldt, int32_t w, int32_t upper, double* dx,
+                         void* stream);
+
+/* dy (m) -= dA (m x k) * dx (k).  Replaces offDiagSolve's block product
+ * (lu.ci:439-456). */
+LU_API int lu_gemv_update(lu_handle h, const double* dA, int64_t lda, int64_t m, int32_t k, const double* dx,
+                          double* dy, void* stream);
+
 /* Kernels this library has launched since it was loaded (all handles). */
 LU_API int64_t lu_launch_count(void);
 

@@ -1,0 +1,169 @@
+"""The 1D block-cyclic multi-GPU LU (charmlu_b200/distributed.py) on CPU:
+world_size 2 and 4 gloo ranks run the driver's distribution (which rank
+factors which panel, the panel and pivot broadcasts, row interchanges across
+every rank's columns, look-ahead ordering, the replicated-b solve) with a
+numpy stand-in for the per-block kernels. Checked against LAPACK getrf
+(scipy): the same pivots, the same L\\U to rounding, x against
+numpy.linalg.solve, and the first singular column reported as lu_factor
+reports it. The kernels themselves are checked on the GPU through the C ABI
+(tests/test_gpu_distributed.py)."""
+import os
+
+import numpy as np
+import pytest
+import scipy.linalg as sl
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+
+class NumpyBlocks:
+    """The per-block operations of CudaBlocks, in numpy on CPU tensors."""
+
+    def __init__(self):
+        self.first_singular = 0
+
+    def panel_factor(self, P, ipiv_out, base):
+        a = P.numpy()
+        m, w = a.shape
+        piv = ipiv_out.numpy()
+        for j in range(w):
+            p = j + int(np.argmax(np.abs(a[j:, j])))  # first maximum, as idamax
+            piv[j] = base + p
+            if p != j:
+                a[[j, p], :] = a[[p, j], :]
+            if a[j, j] == 0.0:
+                if not self.first_singular:
+                    self.first_singular = base + j + 1
+                continue
+            a[j + 1:, j] /= a[j, j]
+            a[j + 1:, j + 1:] -= np.outer(a[j + 1:, j], a[j, j + 1:])
+
+    def apply_pivots(self, A, ncols, ipiv, k0, cnt, skip_b, skip_e, b=None):
+        a = A.numpy()
+        cols = [c for c in range(ncols) if not (skip_b <= c < skip_e)]
+        bv = b.numpy() if b is not None else None
+        piv = ipiv.numpy()
+        for i in range(k0, k0 + cnt):
+            p = int(piv[i])
+            if p != i:
+                if cols:
+                    tmp = a[i, cols].copy()
+                    a[i, cols] = a[p, cols]
+                    a[p, cols] = tmp
+                if bv is not None:
+                    bv[i], bv[p] = bv[p], bv[i]
+
+    def trsm_lower_unit(self, L, B):
+        B.numpy()[:] = sl.solve_triangular(L.numpy(), B.numpy(), lower=True, unit_diagonal=True)
+
+    def gemm_update(self, A, B, C):
+        C.numpy()[:] -= A.numpy() @ B.numpy()
+
+    def trsv_block(self, T, upper, x):
+        x.numpy()[:] = sl.solve_triangular(T.numpy(), x.numpy(), lower=not upper, unit_diagonal=not upper)
+
+    def gemv_update(self, A, x, y):
+        y.numpy()[:] -= A.numpy() @ x.numpy()
+
+    def status(self):
+        return self.first_singular
+
+
+CASES = {
+    2: [(200, 16, True, None), (200, 16, False, None), (64, 8, True, 21), (130, 64, True, None)],
+    4: [(97, 8, True, None), (97, 8, False, None), (40, 4, True, None)],
+}
+
+
+def _matrix(n, seed, zero_col):
+    A = np.random.default_rng(seed).uniform(-0.5, 0.5, (n, n))
+    if zero_col is not None:
+        A[:, zero_col] = 0.0
+    return A
+
+
+def _rank(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    from charmlu_b200.distributed import BlockCyclicLU
+    try:
+        out = []
+        for i, (n, b, la, zero_col) in enumerate(CASES[world]):
+            A = _matrix(n, 100 + i, zero_col)
+            bvec = np.random.default_rng(200 + i).uniform(-0.5, 0.5, n)
+            d = BlockCyclicLU(n, b, blocks=NumpyBlocks(), device="cpu", lookahead=la)
+            loc = d.scatter(torch.from_numpy(A))
+            ipiv = d.factor(loc)
+            LU = d.gather(loc).numpy()
+            x = d.solve(loc, ipiv, torch.from_numpy(bvec)).numpy() if not zero_col else None
+            out.append((LU, ipiv.numpy().copy(), x, d.status_code, d.ncols))
+        q.put((rank, out))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_block_cyclic_lu_gloo_ranks(world):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 31000 + world * 100 + (os.getpid() % 1000)
+    procs = [ctx.Process(target=_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=300) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+    assert sorted(res) == list(range(world))
+    for i, (n, b, la, zero_col) in enumerate(CASES[world]):
+        A = _matrix(n, 100 + i, zero_col)
+        bvec = np.random.default_rng(200 + i).uniform(-0.5, 0.5, n)
+        nb = (n + b - 1) // b
+        # every rank holds its share of the columns and the same replicated results
+        assert sum(res[r][i][4] for r in range(world)) == n
+        for r in range(1, world):
+            assert np.array_equal(res[r][i][0], res[0][i][0]) and np.array_equal(res[r][i][1], res[0][i][1])
+            assert res[r][i][3] == res[0][i][3]
+            if res[0][i][2] is not None:
+                assert np.array_equal(res[r][i][2], res[0][i][2])
+        LU, ipiv, x, status, _ = res[0][i]
+        if zero_col is not None:
+            assert status == zero_col + 1, (status, zero_col)
+            continue
+        assert status == 0
+        lu_ref, piv_ref = sl.lu_factor(A)
+        assert np.array_equal(ipiv, piv_ref.astype(np.int32)), (n, b, la, nb)
+        assert np.abs(LU - lu_ref).max() <= 1e-12 * max(1.0, np.abs(lu_ref).max()) * n
+        xr = np.linalg.solve(A, bvec)
+        assert np.abs(x - xr).max() <= 1e-10 * np.abs(xr).max()
+
+
+def test_layout_owners_and_offsets():
+    """Owned blocks, local column offsets and widths for a ragged last block,
+    without a process group (the layout is pure arithmetic)."""
+    from charmlu_b200.distributed import BlockCyclicLU
+
+    class Fake(BlockCyclicLU):
+        def __init__(self, n, b, rank, world):
+            self.n, self.b, self.rank, self.world = n, b, rank, world
+            self.nb = (n + b - 1) // b
+            self.owned = [j for j in range(self.nb) if j % world == rank]
+            self.col_off, off = {}, 0
+            for j in self.owned:
+                self.col_off[j] = off
+                off += self.width(j)
+            self.ncols = off
+
+    n, b = 1000, 64
+    total = 0
+    for world in (1, 3, 8):
+        cols = []
+        for r in range(world):
+            f = Fake(n, b, r, world)
+            cols.append(f.ncols)
+            assert all(f.owner(j) == r for j in f.owned)
+            assert f._trailing_start(f.nb) == f.ncols
+            for j in f.owned:
+                assert f.col_off[j] % 2 == 0  # 16-byte aligned views in an even-pitch row
+        total = sum(cols)
+        assert total == n
