@@ -16,10 +16,11 @@ in one row-major device matrix. Per step k:
   2. every rank applies the panel's row interchanges to its other columns
      (lu_apply_pivots), solves the U block row of its trailing columns
      (lu_trsm_lower_unit), and updates them (lu_gemm_update);
-  3. with look-ahead, the owner of block column k+1 first updates and
-     factors that panel, then posts its broadcast (asynchronous) before the
-     rest of its update, so the transfer overlaps the GEMM. Every rank posts
-     the same broadcasts in the same order.
+  3. with look-ahead, the owner of block column k+1 first updates that
+     panel's columns, then factors it on a high-priority side stream and
+     posts its broadcast (asynchronous) from there, while the rest of its
+     update runs on the main stream: panel, transfer and GEMM overlap. Every
+     rank posts the same broadcasts in the same order.
 The solve keeps b replicated. Each diagonal block's owner solves it
 (lu_trsv_block), updates the remaining entries (lu_gemv_update) and
 broadcasts them.
@@ -52,10 +53,11 @@ class CudaBlocks:
     Arguments are 2-D views with unit column stride; the leading dimension
     is the row stride."""
 
-    def __init__(self, n, b):
+    def __init__(self, n, b, lookahead=False):
         from . import LUConfig
         self._L = _lib.load()
-        cfg = LUConfig(n, b)
+        # look-ahead: panels use the narrow leaf shape that runs beside an update
+        cfg = LUConfig(n, b, lookahead=lookahead)
         h = ctypes.c_void_p()
         _check(self._L.lu_create(ctypes.byref(cfg.to_c()), ctypes.byref(h)), "lu_create")
         self._h = h
@@ -126,7 +128,12 @@ class BlockCyclicLU:
         self.device = torch.device(device) if device is not None else torch.device(
             "cuda", torch.cuda.current_device())
         self.lookahead = bool(lookahead)
-        self.blocks = blocks if blocks is not None else CudaBlocks(self.n, self.b)
+        self.blocks = blocks if blocks is not None else CudaBlocks(self.n, self.b, lookahead=self.lookahead)
+        # with look-ahead on a GPU, the next panel is factored on a
+        # high-priority stream beside the rest of the update
+        self.side = None
+        if self.lookahead and isinstance(self.blocks, CudaBlocks):
+            self.side = torch.cuda.Stream(device=self.device, priority=-1)
         self.owned = [j for j in range(self.nb) if j % self.world == self.rank]
         self.col_off = {}
         off = 0
@@ -239,8 +246,17 @@ class BlockCyclicLU:
                     # next panel's columns first, then factor and post it
                     w1 = self.width(nxt)
                     self.blocks.gemm_update(L21, U[:, :w1], loc[k1:, t0:t0 + w1])
-                    self._factor_and_pack(loc, ipiv, bufs, nxt)
-                    pending = self._bcast(self._panel_message(bufs, nxt), self.owner(nxt), True)
+                    if self.side is not None:
+                        # the panel's columns are disjoint from the rest of
+                        # the update; the next step waits on the broadcast,
+                        # which follows the panel on the side stream
+                        self.side.wait_stream(torch.cuda.current_stream(self.device))
+                        with torch.cuda.stream(self.side):
+                            self._factor_and_pack(loc, ipiv, bufs, nxt)
+                            pending = self._bcast(self._panel_message(bufs, nxt), self.owner(nxt), True)
+                    else:
+                        self._factor_and_pack(loc, ipiv, bufs, nxt)
+                        pending = self._bcast(self._panel_message(bufs, nxt), self.owner(nxt), True)
                     nxt = None
                     if t0 + w1 < self.ncols:
                         self.blocks.gemm_update(L21, U[:, w1:], loc[k1:, t0 + w1:self.ncols])
