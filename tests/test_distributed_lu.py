@@ -107,7 +107,7 @@ def _rank(rank, world, port, q):
 def test_block_cyclic_lu_gloo_ranks(world):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    port = 31000 + world * 100 + (os.getpid() % 1000)
+    port = 40000 + world * 1000 + (os.getpid() % 1000)  # clear of the other gloo tests' ports
     procs = [ctx.Process(target=_rank, args=(r, world, port, q)) for r in range(world)]
     for p in procs:
         p.start()
