@@ -73,7 +73,7 @@ def load():
         "lu_refine_solve": ([H, P, i64, P, P, ctypes.POINTER(LuRefineInfo), P], ctypes.c_int),
         "lu_refine_solve_host": ([H, P, i64, P, P, ctypes.POINTER(LuRefineInfo), P], ctypes.c_int),
         "lu_panel_factor": ([H, P, i64, i64, i32, P, i64, P], ctypes.c_int),
-        "lu_apply_pivots": ([H, P, i64, i32, P, i64, i32, i32, i32, P, P], ctypes.c_int),
+        "lu_apply_pivots": ([H, P, i64, i64, i32, P, i64, i32, i32, i32, P, P], ctypes.c_int),
         "lu_trsm_lower_unit": ([H, P, i64, i32, P, i64, i64, P], ctypes.c_int),
         "lu_gemm_update": ([H, P, i64, P, i64, P, i64, i64, i64, i64, P], ctypes.c_int),
         "lu_trsv_block": ([H, P, i64, i32, i32, P, P], ctypes.c_int),

@@ -52,7 +52,10 @@ struct PivotList {
   int32_t* src;  // [2*kMaxBatch]
   int32_t* m;    // [1]
 };
-int launch_pivot_compose(const int32_t* ipiv, int k0, int cnt, const PivotList& pl, cudaStream_t s);
+// rows > 0 checks k0 + i <= ipiv[k0 + i] < rows first: a batch that fails
+// moves nothing and records LU_ERR_ARG in st
+int launch_pivot_compose(const int32_t* ipiv, int k0, int cnt, const PivotList& pl, cudaStream_t s, int rows = 0,
+                         DevStatus* st = nullptr);
 // Apply to columns [c_begin, c_end) minus [skip_begin, skip_end); optional
 // vector (rhs) and int permutation carried with the rows.
 template <typename T>

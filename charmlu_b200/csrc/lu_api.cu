@@ -609,16 +609,17 @@ int lu_panel_factor(lu_handle h, double* dP, int64_t ldp, int64_t m, int32_t w, 
   return panel64(c, 0, w, 0, w);
 }
 
-int lu_apply_pivots(lu_handle h, double* dA, int64_t lda, int32_t ncols, const int32_t* d_ipiv, int64_t k0,
-                    int32_t cnt, int32_t skip_b, int32_t skip_e, double* db, void* stream) {
-  if (!h || !d_ipiv || ncols < 0 || cnt < 0 || k0 < 0 || k0 + cnt > ((int64_t)1 << 31) - 1) return LU_ERR_ARG;
+int lu_apply_pivots(lu_handle h, double* dA, int64_t lda, int64_t m, int32_t ncols, const int32_t* d_ipiv,
+                    int64_t k0, int32_t cnt, int32_t skip_b, int32_t skip_e, double* db, void* stream) {
+  if (!h || !d_ipiv || ncols < 0 || cnt < 0 || k0 < 0 || m < 1 || m > ((int64_t)1 << 31) - 1 || k0 + cnt > m)
+    return LU_ERR_ARG;
   if (ncols > 0) LUB_TRY(check_view(dA, lda, ncols));
   LUB_TRY(ensure_kernels_init());
   cudaStream_t s = (cudaStream_t)stream;
   Prof pf(h, s, LU_PH_LASWP);
   for (int off = 0; off < cnt; off += 512) {
     const int sub = std::min(512, cnt - off);
-    LUB_TRY(launch_pivot_compose(d_ipiv, (int)k0 + off, sub, h->plist, s));
+    LUB_TRY(launch_pivot_compose(d_ipiv, (int)k0 + off, sub, h->plist, s, (int)m, h->st));
     LUB_TRY(launch_pivot_apply<double>(dA, lda, 0, ncols, skip_b, skip_e, h->plist, 2 * sub, db, nullptr, s));
   }
   return LU_OK;

@@ -74,10 +74,28 @@ __device__ int compose_batch(const int32_t* ipiv, int k0, int cnt, int* p, int* 
   return *s_m;
 }
 
-__global__ void __launch_bounds__(1024) pivot_compose_kernel(const int32_t* ipiv, int k0, int cnt, PivotList pl) {
+// rows > 0: the pivots must satisfy k0 + i <= p_i < rows (and k0 + cnt <=
+// rows); otherwise the list is left empty, so nothing moves, and LU_ERR_ARG
+// is recorded in st.
+__global__ void __launch_bounds__(1024) pivot_compose_kernel(const int32_t* ipiv, int k0, int cnt, PivotList pl,
+                                                            int rows, DevStatus* st) {
   __shared__ int p[kMaxBatch], nxt[kMaxBatch], lb[kMaxBatch];
   __shared__ int dst[2 * kMaxBatch], src[2 * kMaxBatch];
   __shared__ int s_m;
+  if (rows > 0) {
+    int bad = k0 + cnt > rows;
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+      const int pi = ipiv[k0 + i];
+      bad |= (pi < k0 + i) | (pi >= rows);
+    }
+    if (__syncthreads_or(bad)) {
+      if (threadIdx.x == 0) {
+        *pl.m = 0;
+        if (st) dev_fail(st, LU_ERR_ARG, 301);
+      }
+      return;
+    }
+  }
   const int m = compose_batch(ipiv, k0, cnt, p, nxt, lb, dst, src, &s_m);
   for (int i = threadIdx.x; i < m; i += blockDim.x) {
     pl.dst[i] = dst[i];
@@ -221,10 +239,11 @@ __global__ void __launch_bounds__(1024) ipiv_apply_vector_kernel(const int32_t* 
 
 }  // namespace
 
-int launch_pivot_compose(const int32_t* ipiv, int k0, int cnt, const PivotList& pl, cudaStream_t s) {
+int launch_pivot_compose(const int32_t* ipiv, int k0, int cnt, const PivotList& pl, cudaStream_t s, int rows,
+                         DevStatus* st) {
   if (cnt <= 0) return LU_OK;
   if (cnt > kMaxBatch) return LU_ERR_ARG;
-  pivot_compose_kernel<<<1, 1024, 0, s>>>(ipiv, k0, cnt, pl);
+  pivot_compose_kernel<<<1, 1024, 0, s>>>(ipiv, k0, cnt, pl, rows, st);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }

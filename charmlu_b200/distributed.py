@@ -83,7 +83,8 @@ class CudaBlocks:
                "lu_panel_factor")
 
     def apply_pivots(self, A, ncols, ipiv, k0, cnt, skip_b, skip_e, b=None):
-        _check(self._L.lu_apply_pivots(self._h, _ptr(A) if ncols > 0 else None, A.stride(0) if ncols > 0 else 2,
+        m = A.shape[0] if ncols > 0 else b.shape[0]
+        _check(self._L.lu_apply_pivots(self._h, _ptr(A) if ncols > 0 else None, A.stride(0) if ncols > 0 else 2, m,
                                        ncols, _ptr(ipiv), k0, cnt, skip_b, skip_e,
                                        _ptr(b) if b is not None else None, self._s()), "lu_apply_pivots")
 

@@ -292,13 +292,16 @@ LU_API int lu_panel_factor(lu_handle h, double* dP, int64_t ldp, int64_t m, int3
                            int64_t base, void* stream);
 
 /* Row interchanges d_ipiv[k0 .. k0+cnt) (device, global 0-based rows, in
- * order) on columns [0, ncols) of dA, except the columns [skip_b, skip_e)
- * that already hold them (the factored panel); db (optional, device) is
- * permuted too.  dA must have every row the pivots name.  Replaces the
- * pivot batches applied to the other block columns and to b
- * (sendPendingPivots / applySwap, lu.C:46-169; pivotBatch, lu.ci:92-123). */
-LU_API int lu_apply_pivots(lu_handle h, double* dA, int64_t lda, int32_t ncols, const int32_t* d_ipiv, int64_t k0,
-                           int32_t cnt, int32_t skip_b, int32_t skip_e, double* db, void* stream);
+ * order: row k0+i swaps with d_ipiv[k0+i]) on columns [0, ncols) of the
+ * m-row matrix dA, except the columns [skip_b, skip_e) that already hold
+ * them (the factored panel); db (optional, device, m entries) is permuted
+ * too.  Each pivot must satisfy k0+i <= d_ipiv[k0+i] < m, as getrf's do; a
+ * batch of up to 512 that does not is left unapplied and LU_ERR_ARG is
+ * recorded for lu_status.  Replaces the pivot batches applied to the other
+ * block columns and to b (sendPendingPivots / applySwap, lu.C:46-169;
+ * pivotBatch, lu.ci:92-123). */
+LU_API int lu_apply_pivots(lu_handle h, double* dA, int64_t lda, int64_t m, int32_t ncols, const int32_t* d_ipiv,
+                           int64_t k0, int32_t cnt, int32_t skip_b, int32_t skip_e, double* db, void* stream);
 
 /* dB (w x ncols) <- L^{-1} dB with L the unit lower triangle of dL (w x w).
  * Replaces LUBlk::computeU (lu.C:180-189). */

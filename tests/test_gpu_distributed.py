@@ -111,6 +111,22 @@ def test_panel_factor_and_pivots_match_lapack(cuda_dev, m, w, base):
 _PORTS = iter(range(33000 + (os.getpid() % 500) * 8, 33000 + (os.getpid() % 500) * 8 + 8))
 
 
+def test_apply_pivots_rejects_rows_outside_the_matrix(cuda_dev):
+    """A pivot naming a row at or past m (or before its own position) is
+    caught before anything moves: the batch is left unapplied and the status
+    word reports LU_ERR_ARG."""
+    import charmlu_b200 as lu
+    bl = _blocks(1024, 64)
+    m = 100
+    A = _even(m, 40, 15)
+    A0 = A.clone()
+    ipiv = torch.arange(8, dtype=torch.int32, device="cuda")
+    ipiv[3] = m  # one past the last row
+    bl.apply_pivots(A, 40, ipiv, 0, 8, 0, 0)
+    assert bl.status() == lu.LU_ERR_ARG
+    assert torch.equal(A, A0)
+
+
 @pytest.fixture()
 def one_rank_group():
     """A one-rank NCCL process group (a fresh store port per test)."""
