@@ -83,6 +83,8 @@ class CudaBlocks:
                "lu_panel_factor")
 
     def apply_pivots(self, A, ncols, ipiv, k0, cnt, skip_b, skip_e, b=None):
+        if ncols <= 0 and b is None:
+            return
         m = A.shape[0] if ncols > 0 else b.shape[0]
         _check(self._L.lu_apply_pivots(self._h, _ptr(A) if ncols > 0 else None, A.stride(0) if ncols > 0 else 2, m,
                                        ncols, _ptr(ipiv), k0, cnt, skip_b, skip_e,
@@ -237,7 +239,8 @@ class BlockCyclicLU:
                 panel = msg[:m * self.ldp].view(m, self.ldp)[:, :kw]
                 Lkk, L21 = panel[:kw], panel[kw:]
                 skip = (0, 0)
-            self.blocks.apply_pivots(loc, self.ncols, ipiv, k0, kw, skip[0], skip[1])
+            if self.ncols > 0:  # a rank may own no block when world > nb
+                self.blocks.apply_pivots(loc, self.ncols, ipiv, k0, kw, skip[0], skip[1])
             t0 = self._trailing_start(k)
             nxt = k + 1 if k + 1 < self.nb else None
             if t0 < self.ncols and k1 < n:

@@ -70,9 +70,13 @@ class NumpyBlocks:
         return self.first_singular
 
 
+# (n, b, look-ahead, zero column): ragged last blocks, ranks that own no
+# block (n <= b at world 2; 3 blocks at world 4), a singular matrix
 CASES = {
-    2: [(200, 16, True, None), (200, 16, False, None), (64, 8, True, 21), (130, 64, True, None)],
-    4: [(97, 8, True, None), (97, 8, False, None), (40, 4, True, None)],
+    2: [(200, 16, True, None), (200, 16, False, None), (64, 8, True, 21), (130, 64, True, None),
+        (6, 8, True, None)],
+    4: [(97, 8, True, None), (97, 8, False, None), (40, 4, True, None), (20, 8, True, None),
+        (20, 8, False, None)],
 }
 
 
