@@ -310,6 +310,7 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
         cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->evP, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->evN, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->evR, cudaEventDisableTiming) != cudaSuccess ||
         cudaStreamCreateWithFlags(&h->sG, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->evG0, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->evG1, cudaEventDisableTiming) != cudaSuccess)
@@ -327,6 +328,7 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
   if (const char* e = getenv("LU_B200_GEMM_RESERVE")) h->gemm_reserve = std::max(0, atoi(e));
   if (const char* e = getenv("LU_B200_GEMM_HELPER")) h->gemm_helper = atoi(e) != 0;
   if (const char* e = getenv("LU_B200_PANEL_TC")) h->panel_tc = atoi(e) != 0;
+  if (const char* e = getenv("LU_B200_LA_SPLIT")) h->la_split = atoi(e) != 0;
   if (const char* e = getenv("LU_B200_STAGE_BYTES")) h->stage_bytes = std::max<size_t>(1 << 16, strtoull(e, nullptr, 10));
   if (const char* e = getenv("LU_B200_RESIDENT_BYTES")) h->resident_cap = strtoull(e, nullptr, 10);
   if (s == LU_OK) s = h->alloc(&h->perm, n);
@@ -353,6 +355,7 @@ int lu_destroy(lu_handle h) {
   if (h->evFork) cudaEventDestroy(h->evFork);
   if (h->evP) cudaEventDestroy(h->evP);
   if (h->evN) cudaEventDestroy(h->evN);
+  if (h->evR) cudaEventDestroy(h->evR);
   if (h->sP) cudaStreamDestroy(h->sP);
   for (auto& g : h->gslot)
     if (g.exec) cudaGraphExecDestroy(g.exec);

@@ -191,6 +191,35 @@ int build_operands(lu_handle h, const Ctx32& c, int k0, int kw, int k1, int rest
   return LU_OK;
 }
 
+// Pairs-layout operands of step k for the update of trailing columns
+// [u0, u0+ncols) only: the U12^T rows of those columns (and, with with_l,
+// all of L21). amax[0], amax[1] receive max|L21| and max|U12| over those
+// columns, and set the scales; a later part with its own amax pair scales
+// its U rows by its own maximum (L21's maximum is the same number). The
+// tensor maps cover every trailing column, as build_operands' do.
+int build_operands_part(lu_handle h, const Ctx32& c, int k0, int kw, int k1, int rest, int u0, int ncols,
+                        bool with_l, unsigned* amax, CUtensorMap* mapL, CUtensorMap* mapU, int* K, int* kpart,
+                        cudaStream_t s) {
+  const float* L21 = c.A + (int64_t)k1 * c.ld + k0;
+  const float* U12 = c.A + (int64_t)k0 * c.ld + k1 + u0;
+  const int kps = (kw + 63) & ~63;
+  *K = kps;
+  *kpart = kps;
+  {
+    Prof pf(h, s, LU_PH_OTHER);
+    LUB_TRY(launch_panel_absmax(L21, c.ld, rest, kw, U12, c.ld, ncols, amax, s));
+    if (with_l)
+      LUB_TRY(launch_split_rows<__half>(L21, c.ld, reinterpret_cast<__half*>(h->Lb), h->ldk, rest, kw, 2, 0x2u, amax,
+                                        0, s, kps));
+    LUB_TRY(launch_split_transpose<__half>(U12, c.ld, reinterpret_cast<__half*>(h->Ub) + (int64_t)u0 * h->ldk,
+                                           h->ldk, kw, ncols, 2, 0x2u, amax, 1, s, kps));
+  }
+  LUB_TRY(encode_tmap_2d(mapL, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, h->Lb, 2 * kps, rest, h->ldk * 2, 64, 128,
+                         CU_TENSOR_MAP_SWIZZLE_128B));
+  return encode_tmap_2d(mapU, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, h->Ub, 2 * kps, rest, h->ldk * 2, 64, 256,
+                        CU_TENSOR_MAP_SWIZZLE_128B);
+}
+
 // C(k1.., c0..c0+ncols) -= L21 * U12[:, u0..u0+ncols] on the tensor cores
 // (reserve: SMs left free for a panel running beside it).  K and kpart as
 // from build_operands; flops are counted as executed on the panel's kw
@@ -200,8 +229,8 @@ int build_operands(lu_handle h, const Ctx32& c, int k0, int kw, int k1, int rest
 // a phase, since the main launch's span covers the whole product).
 int lowp_gemm(lu_handle h, const CUtensorMap& mapL, const CUtensorMap& mapU, const CUtensorMap& mapC, int k1,
               int rest, int u0, int ncols, int K, int kpart, int kw, bool bf16, cudaStream_t s, int reserve = 0,
-              unsigned* tile_ctr = nullptr, int helper_ctas = 0) {
-  const unsigned* amax = bf16 ? nullptr : h->amax;
+              unsigned* tile_ctr = nullptr, int helper_ctas = 0, const unsigned* amax_in = nullptr) {
+  const unsigned* amax = bf16 ? nullptr : (amax_in ? amax_in : h->amax);
   if (helper_ctas > 0)
     return launch_gemm_lowp_persistent(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, K, bf16, amax, h->st,
                                        h->spin, helper_ctas, s, kpart, tile_ctr);
@@ -211,6 +240,50 @@ int lowp_gemm(lu_handle h, const CUtensorMap& mapL, const CUtensorMap& mapU, con
     return launch_gemm_lowp_persistent(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, K, bf16, amax, h->st,
                                        h->spin, std::max(1, h->gemm_ctas - reserve), s, kpart, tile_ctr);
   return launch_gemm_bf16_tc(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, K, bf16, amax, h->st, h->spin, s);
+}
+
+// One look-ahead step with the next panel's columns first (pairs layout):
+// on the main stream the interchanges, U solve, operands and update of
+// panel k+1's nw columns; then panel k+1 starts on the panel stream while
+// the main stream does the same for every other column (interchanges on
+// the left columns and the row permutation included). The rest's U rows
+// get their own scale (h->amax[2..3]); the helper launch, if any, waits
+// for them. Per column the interchanges, U solve and products are the same
+// operations as in the one-pass schedule.
+int factor_mixed_split_step(lu_handle h, Ctx32& c, Ctx32& cp, const CUtensorMap& mapC, int k0, int kw,
+                            cudaStream_t s) {
+  const int n = (int)h->cfg.n, B = h->cfg.block_size;
+  const int k1 = k0 + kw, rest = n - k1, nw = std::min(B, rest);
+  LUB_TRY(pivots_apply_f32(c, k0, kw, k1, k1 + nw, 0, 0, nullptr));
+  LUB_TRY(trsm32(c, k0, kw, k0, k1, nw));
+  CUtensorMap mapL, mapU;
+  int K = 0, kpart = 0;
+  LUB_TRY(build_operands_part(h, c, k0, kw, k1, rest, 0, nw, true, h->amax, &mapL, &mapU, &K, &kpart, s));
+  LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, 0, nw, K, kpart, kw, false, s));  // next panel's columns
+  LUB_CUDA(cudaEventRecord(h->evN, s));
+  LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evN, 0));
+  LUB_TRY(panel32(cp, k1, nw, k1, nw));
+  // every other column: the left L columns, and the trailing ones past the
+  // next panel (the panel's own columns are being factored beside this)
+  LUB_TRY(pivots_apply_f32(c, k0, kw, 0, n, k0, k1 + nw, h->perm));
+  if (rest == nw) {
+    LUB_CUDA(cudaEventRecord(h->evP, h->sP));
+    return LU_OK;
+  }
+  LUB_TRY(trsm32(c, k0, kw, k0, k1 + nw, rest - nw));
+  CUtensorMap mapL2, mapU2;
+  LUB_TRY(build_operands_part(h, c, k0, kw, k1, rest, nw, rest - nw, false, h->amax + 2, &mapL2, &mapU2, &K, &kpart,
+                              s));
+  unsigned* ctr = (h->gemm_helper && h->gemm_ctas > 0 && h->gemm_reserve > 0) ? h->take_counter() : nullptr;
+  if (ctr) {
+    LUB_CUDA(cudaEventRecord(h->evR, s));
+    LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evR, 0));
+    LUB_TRY(lowp_gemm(h, mapL2, mapU2, mapC, k1, rest, nw, rest - nw, K, kpart, kw, false, h->sP, 0, ctr,
+                      h->gemm_reserve, h->amax + 2));
+  }
+  LUB_CUDA(cudaEventRecord(h->evP, h->sP));
+  return lowp_gemm(h, mapL2, mapU2, mapC, k1, rest, nw, rest - nw, K, kpart, kw, false, s, h->gemm_reserve, ctr, 0,
+                   h->amax + 2);
 }
 
 // LU of h->A32 in place: FP32 panels/TRSM, low-precision tcgen05 trailing
@@ -249,9 +322,14 @@ int factor_mixed(lu_handle h, cudaStream_t s) {
   LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evFork, 0));
   LUB_TRY(panel32(cp, 0, std::min(B, n), 0, std::min(B, n)));
   LUB_CUDA(cudaEventRecord(h->evP, h->sP));
+  const bool split = h->la_split && h->pairs && !bf16;
   for (int k0 = 0; k0 < n; k0 += B) {
     const int kw = std::min(B, n - k0), k1 = k0 + kw, rest = n - k1;
     LUB_CUDA(cudaStreamWaitEvent(s, h->evP, 0));
+    if (split && rest > 0) {
+      LUB_TRY(factor_mixed_split_step(h, c, cp, mapC, k0, kw, s));
+      continue;
+    }
     LUB_TRY(pivots_apply_f32(c, k0, kw, 0, n, k0, k1, h->perm));
     if (rest <= 0) continue;
     LUB_TRY(trsm32(c, k0, kw, k0, k1, rest));
