@@ -671,6 +671,15 @@ int lu_trsv_block(lu_handle h, const double* dT, int64_t ldt, int32_t w, int32_t
   return launch_trsv<double>(dT, ldt, w, dx, upper ? 1 : 0, h->trsv_flags, h->trsv_ticket, h->st, h->spin, s);
 }
 
+int lu_copy_2d(void* dst, int64_t dpitch, const void* src, int64_t spitch, int64_t width, int64_t rows,
+               void* stream) {
+  if (!dst || !src || width < 0 || rows < 0 || dpitch < width || spitch < width) return LU_ERR_ARG;
+  if (width == 0 || rows == 0) return LU_OK;
+  LUB_CUDA(cudaMemcpy2DAsync(dst, (size_t)dpitch, src, (size_t)spitch, (size_t)width, (size_t)rows,
+                             cudaMemcpyDefault, (cudaStream_t)stream));
+  return LU_OK;
+}
+
 int lu_gemv_update(lu_handle h, const double* dA, int64_t lda, int64_t m, int32_t k, const double* dx, double* dy,
                    void* stream) {
   if (!h || !dx || !dy || m < 0 || k < 0 || m > ((int64_t)1 << 31) - 1) return LU_ERR_ARG;

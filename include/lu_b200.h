@@ -324,6 +324,15 @@ LU_API int lu_trsv_block(lu_handle h, const double* dT, int64_t ldt, int32_t w, 
 LU_API int lu_gemv_update(lu_handle h, const double* dA, int64_t lda, int64_t m, int32_t k, const double* dx,
                           double* dy, void* stream);
 
+/* Copy a rows x width-byte block between host and device memory (either
+ * direction; pitches in bytes), asynchronous on stream.  Host memory should
+ * be page-locked for the copy to overlap kernels.  Used by the out-of-core
+ * FP64 driver (charmlu_b200/ooc.py) to move column panels of a row-major
+ * host matrix; no reference counterpart (the reference keeps every block
+ * in memory, scheduler.C:46-47 only limits how many are in flight). */
+LU_API int lu_copy_2d(void* dst, int64_t dpitch, const void* src, int64_t spitch, int64_t width, int64_t rows,
+                      void* stream);
+
 /* Kernels this library has launched since it was loaded (all handles). */
 LU_API int64_t lu_launch_count(void);
 
