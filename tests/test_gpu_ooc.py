@@ -29,9 +29,10 @@ def test_out_of_core_factor_and_solve(cuda_dev, n, w):
     LU = host.to("cuda")
     assert (LU - ref).abs().max().item() <= 1e-12 * n * ref.abs().max().item()
     assert s.residual(A, x, rhs)["r_hpl"] < 16
+    # two backward-stable solutions differ by about kappa * sqrt(n) * eps
     xr = rhs.clone()
     s.solve(ref, ipiv_ref, xr)
-    assert (x - xr).abs().max().item() <= 1e-10 * xr.abs().max().item()
+    assert (x - xr).abs().max().item() <= 1e-8 * xr.abs().max().item()
 
 
 def test_out_of_core_singular_column(cuda_dev):
