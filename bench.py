@@ -598,6 +598,62 @@ def run_blockcyclic(args, rank, world):
     return 0
 
 
+def run_ooc64(args, rank, world):
+    """Out-of-core FP64 LU + solve (charmlu_b200.ooc.OutOfCoreLU): the matrix
+    in pinned host memory, column panels streamed through the GPU; at
+    --ooc-n (default 65536, beside the in-core lu_factor_solve of the same
+    matrix when that fits) one factor + solve timed with CUDA events, r_hpl
+    checked against a regenerated copy on the device when it fits, else
+    skipped."""
+    import torch
+    import charmlu_b200 as lu
+    from charmlu_b200.ooc import OutOfCoreLU
+    if rank != 0:
+        return 0
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    n, b = args.ooc_n, args.block
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 0
+    if avail < 1.15 * 8 * n * n:
+        print(json.dumps({"workload": "ooc64", "n": n, "skipped": f"host memory {avail / 1e9:.0f} GB"}))
+        return 0
+    host = torch.empty(n, n, dtype=torch.float64, pin_memory=True)
+    chunk = max(1, (1 << 30) // (8 * n))
+    for r0 in range(0, n, chunk):
+        r = min(chunk, n - r0)
+        host[r0:r0 + r].copy_(lu.generate_uniform(r, n, seed=42, stream_id=2000 + r0 // chunk, device=dev))
+    rhs = lu.generate_uniform(n, 1, seed=42, stream_id=1, device=dev).view(-1)
+    ooc = OutOfCoreLU(n, b=b)
+    orig = host.clone() if 8 * n * n * 1.6 < torch.cuda.mem_get_info(dev)[0] else None
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    ipiv = ooc.factor(host)
+    x = ooc.solve(host, ipiv, rhs)
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1)
+    row = {"workload": "ooc64", "n": n, "panel_width": ooc.w, "ms": t, "tflops": flops_lu(n) / (t / 1e3) / 1e12,
+           "status": ooc.status_code, "fp64_matrix_gb_in_host_memory": 8 * n * n / 1e9,
+           "device_panels_gb": 3 * 8 * n * ooc.w / 1e9}
+    if orig is not None:
+        A = orig.to(dev)
+        row["r_hpl"] = lu.LUSolver(lu.LUConfig(n, b)).residual(A, x, rhs)["r_hpl"]
+        s = lu.LUSolver(lu.LUConfig(n, b, lookahead=True))
+        xr = rhs.clone()
+        e0.record()
+        s.factor_solve(A, xr)
+        e1.record()
+        torch.cuda.synchronize()
+        row["in_core_ms"] = e0.elapsed_time(e1)
+    print(json.dumps(row), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -617,7 +673,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="lu", choices=["lu", "batched", "ksweep", "adjoint", "ooc",
-                                                         "blockcyclic"])
+                                                         "blockcyclic", "ooc64"])
     ap.add_argument("--ooc-n", type=int, default=65536)
     ap.add_argument("--adjoint-n", type=int, default=4096)
     ap.add_argument("--adjoint-mixed-n", type=int, default=32768)
@@ -642,6 +698,8 @@ def main():
         return run_ooc(args, rank, world)
     if args.workload == "blockcyclic":
         return run_blockcyclic(args, rank, world)
+    if args.workload == "ooc64":
+        return run_ooc64(args, rank, world)
 
     import torch
     import charmlu_b200 as lu
