@@ -151,6 +151,18 @@ def test_singular_column_reports_info(cuda_dev):
     assert info_ref == 71 and st == 71
 
 
+@pytest.mark.parametrize("lookahead", [False, True])
+def test_exact_tie_lowest_row_wins(cuda_dev, lookahead):
+    """|a_i0| = 1 exactly at rows 10, 1000 and 3000 (signs -, +, -), rows
+    held by different CTAs of the panel grid: the pivot is row 10, as in the
+    oracle (lowest global row wins an exact tie)."""
+    A = oracle.gen_matrix(4096, 3)
+    A[10, 0], A[1000, 0], A[3000, 0] = -1.0, 1.0, -1.0
+    _, _, ipiv_ref, _, _ = oracle.lu_factor(A, b=256)
+    s, Ag, ipiv, _, st = _gpu_factor(A, 256, lookahead=lookahead)
+    assert st == 0 and int(ipiv[0]) == 10 and ipiv_ref[0] == 10
+
+
 def test_reference_threshold_singularity(cuda_dev):
     lu = _lu()
     n, b = 128, 32

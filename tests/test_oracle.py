@@ -91,6 +91,23 @@ def test_oracle_singular_reports_info():
     assert info2 > 0
 
 
+def _tied_first_column(n, seed):
+    """|a_i0| = 1 exactly at rows 10, 1000 and 3000 (signs -, +, -); every
+    other entry of the matrix is in [-0.5, 0.5)."""
+    A = oracle.gen_matrix(n, seed)
+    A[10, 0], A[1000, 0], A[3000, 0] = -1.0, 1.0, -1.0
+    return A
+
+
+def test_oracle_tie_lowest_row_wins():
+    """Exact ties in |a_ij| go to the lowest global row (the reference's
+    strict '>' inside a block; across blocks its order depends on message
+    arrival, which the oracle fixes to lowest row)."""
+    A = _tied_first_column(4096, 3)
+    LU, ipiv, _, _, info = oracle.lu_factor(A, b=256)
+    assert info == 0 and ipiv[0] == 10
+
+
 def test_oracle_apply_pivots_roundtrip():
     n = 300
     A = oracle.gen_matrix(n, 9)
