@@ -15,11 +15,13 @@ import dataclasses
 import torch
 
 from . import _lib
-from ._lib import (LU_ERR_ARG, LU_ERR_NOCONV, LU_ERR_TIMEOUT, LU_ERR_UNSUPPORTED, LU_IR_CLASSIC, LU_IR_GMRES, LU_OK,
-                   LU_PREC_BF16, LU_PREC_FP16S, LU_PREC_FP16X3, LU_PREC_FP32, LU_PREC_FP64)
+from ._lib import (LU_ERR_ARG, LU_ERR_NOCONV, LU_ERR_TIMEOUT, LU_ERR_UNSUPPORTED, LU_IR_CLASSIC, LU_IR_GMRES,
+                   LU_LAYOUT_COL, LU_LAYOUT_ROW, LU_OK, LU_PREC_BF16, LU_PREC_FP16S, LU_PREC_FP16X3, LU_PREC_FP32,
+                   LU_PREC_FP64)
 
 __all__ = ["LUConfig", "LUSolver", "LUError", "generate_uniform", "matgen", "status_string",
-           "LU_PREC_FP64", "LU_PREC_BF16", "LU_PREC_FP16S", "LU_PREC_FP16X3", "LU_PREC_FP32", "LU_IR_CLASSIC", "LU_IR_GMRES"]
+           "LU_PREC_FP64", "LU_PREC_BF16", "LU_PREC_FP16S", "LU_PREC_FP16X3", "LU_PREC_FP32", "LU_IR_CLASSIC", "LU_IR_GMRES",
+           "LU_LAYOUT_ROW", "LU_LAYOUT_COL", "transpose_square"]
 
 EPS = 2.220446049250313e-16
 
@@ -72,6 +74,7 @@ class LUConfig:
     ir_target: float = 16.0
     sing_threshold: float = 0.0        # reference: 100*eps aborts (lu.ci:339)
     spin_limit: int = 0
+    layout: int = LU_LAYOUT_ROW        # LU_LAYOUT_COL: factor / factor_solve take column-major A
 
     def to_c(self):
         c = _lib.LuConfig()
@@ -87,6 +90,7 @@ class LUConfig:
         c.ir_target = float(self.ir_target)
         c.sing_threshold = float(self.sing_threshold)
         c.spin_limit = int(self.spin_limit)
+        c.layout = int(self.layout)
         return c
 
 
@@ -135,6 +139,10 @@ class LUSolver:
     def _check_matrix(self, A):
         _require_cuda(A, torch.float64, "A")
         n = self.n
+        if self.cfg.layout == LU_LAYOUT_COL:  # column-major: unit row stride, pitch = column stride
+            if A.dim() != 2 or A.shape[0] != n or A.shape[1] != n or A.stride(0) != 1:
+                raise LUError(LU_ERR_ARG, "A must be n x n and column-major (unit row stride)")
+            return A.stride(1)
         if A.dim() != 2 or A.shape[0] != n or A.shape[1] != n or A.stride(1) != 1:
             raise LUError(LU_ERR_ARG, "A must be n x n with unit column stride")
         return A.stride(0)
@@ -296,6 +304,18 @@ class LUSolver:
 def launch_count():
     """Kernels liblu_b200 has launched since it was loaded."""
     return int(_lib.load().lu_launch_count())
+
+
+def transpose_square(A, stream=None):
+    """A <- A^T in place for a square float64 CUDA matrix with unit column
+    stride (lu_transpose_square): converts the storage between row- and
+    column-major."""
+    _require_cuda(A, torch.float64, "A")
+    if A.dim() != 2 or A.shape[0] != A.shape[1] or A.stride(1) != 1:
+        raise LUError(LU_ERR_ARG, "A must be square with unit column stride")
+    _check(_lib.load().lu_transpose_square(_ptr(A), A.shape[0], A.stride(0), _stream(stream)),
+           "lu_transpose_square")
+    return A
 
 
 def generate_uniform(rows, cols, seed=42, stream_id=0, device="cuda", out=None):

@@ -14,6 +14,7 @@ LU_ERR_ARG, LU_ERR_CUDA, LU_ERR_TIMEOUT, LU_ERR_NONFINITE = -1, -2, -3, -4
 LU_ERR_NOCONV, LU_ERR_ALIGN, LU_ERR_NOMEM, LU_ERR_UNSUPPORTED = -5, -6, -7, -8
 LU_PREC_FP64, LU_PREC_BF16, LU_PREC_FP16S, LU_PREC_FP16X3, LU_PREC_FP32 = 0, 1, 2, 3, 4
 LU_IR_CLASSIC, LU_IR_GMRES = 0, 1
+LU_LAYOUT_ROW, LU_LAYOUT_COL = 0, 1
 
 # every symbol the header declares (checked by the CPU test suite)
 EXPORTS = [
@@ -23,7 +24,7 @@ EXPORTS = [
     "lu_profile", "lu_phase_times", "lu_launch_count", "lu_solve_noalloc",
     "lu_batched_work_bytes", "lu_batched_set_tuning", "lu_refine_factor", "lu_refine_apply",
     "lu_refine_adjoint", "lu_panel_factor", "lu_apply_pivots", "lu_trsm_lower_unit", "lu_gemm_update",
-    "lu_trsv_block", "lu_gemv_update", "lu_copy_2d",
+    "lu_trsv_block", "lu_gemv_update", "lu_copy_2d", "lu_transpose_square",
 ]
 PHASES = ["panel", "laswp", "trsm", "gemm", "gemm_inner", "solve", "other"]
 
@@ -32,7 +33,7 @@ class LuConfig(ctypes.Structure):
     _fields_ = [
         ("n", ctypes.c_int64), ("block_size", ctypes.c_int32), ("pivot_batch", ctypes.c_int32),
         ("precision", ctypes.c_int32), ("lookahead", ctypes.c_int32), ("use_graph", ctypes.c_int32),
-        ("ir_mode", ctypes.c_int32), ("ir_max_iter", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("ir_mode", ctypes.c_int32), ("ir_max_iter", ctypes.c_int32), ("layout", ctypes.c_int32),
         ("sing_threshold", ctypes.c_double), ("ir_target", ctypes.c_double), ("spin_limit", ctypes.c_int64),
     ]
 
@@ -79,6 +80,7 @@ def load():
         "lu_trsv_block": ([H, P, i64, i32, i32, P, P], ctypes.c_int),
         "lu_gemv_update": ([H, P, i64, i64, i32, P, P, P], ctypes.c_int),
         "lu_copy_2d": ([P, i64, P, i64, i64, i64, P], ctypes.c_int),
+        "lu_transpose_square": ([P, i64, i64, P], ctypes.c_int),
         "lu_adjoint": ([H, P, i64, P, P, i64, P, i64, i64, P, i64, P, i64, P], ctypes.c_int),
         "lu_refine_factor": ([H, P, i64, P], ctypes.c_int),
         "lu_refine_apply": ([H, P, i64, i32, P, i64, P, i64, i64, ctypes.POINTER(LuRefineInfo), P], ctypes.c_int),

@@ -113,6 +113,8 @@ struct ResidualAccum {  // non-negative doubles stored as ordered bit patterns
 };
 int launch_residual_f64(const double* A, int64_t lda, int n, const double* x, const double* b, double* r,
                         ResidualAccum* acc, cudaStream_t s);
+// A <- A^T in place (n x n, row pitch lda)
+int launch_transpose_inplace(double* A, int64_t lda, int n, cudaStream_t s);
 // y[0:m] -= A[0:m, 0:k] x (one warp per row)
 int launch_gemv_sub(const double* A, int64_t lda, int m, int k, const double* x, double* y, cudaStream_t s);
 // the same for rows row0 .. row0 + rows - 1 only (Arows = their first row);

@@ -276,6 +276,8 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
   if (!cfg || !out) return LU_ERR_ARG;
   if (cfg->n <= 0 || cfg->n > (int64_t)1 << 30 || cfg->block_size < 2 || (cfg->block_size & 1)) return LU_ERR_ARG;
   if (cfg->precision < LU_PREC_FP64 || cfg->precision > LU_PREC_FP16X3) return LU_ERR_ARG;
+  if (cfg->layout != LU_LAYOUT_ROW && cfg->layout != LU_LAYOUT_COL) return LU_ERR_ARG;
+  if (cfg->layout == LU_LAYOUT_COL && cfg->precision != LU_PREC_FP64) return LU_ERR_UNSUPPORTED;
   LUB_TRY(ensure_kernels_init());
   lu_handle h = new lu_handle_s();
   h->cfg = *cfg;
@@ -385,7 +387,18 @@ int lu_status(lu_handle h, void* stream) {
 int lu_factor(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double* rhs, void* stream) {
   if (!h) return LU_ERR_ARG;
   if (h->cfg.precision != LU_PREC_FP64) return LU_ERR_UNSUPPORTED;
-  return factor_f64(h, dA, lda, ipiv, rhs, (cudaStream_t)stream);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (h->cfg.layout != LU_LAYOUT_COL) return factor_f64(h, dA, lda, ipiv, rhs, s);
+  LUB_TRY(check_common(h, dA, lda));
+  const int n = (int)h->cfg.n;
+  LUB_TRY(launch_transpose_inplace(dA, lda, n, s));
+  LUB_TRY(factor_f64(h, dA, lda, ipiv, rhs, s));
+  return launch_transpose_inplace(dA, lda, n, s);
+}
+
+int lu_transpose_square(double* dA, int64_t n, int64_t lda, void* stream) {
+  if (!dA || n < 0 || lda < n || n > ((int64_t)1 << 31) - 1) return LU_ERR_ARG;
+  return launch_transpose_inplace(dA, lda, (int)n, (cudaStream_t)stream);
 }
 
 // n x nrhs staging block owned by the handle
@@ -418,6 +431,7 @@ static int solve_trans_multi(lu_handle h, const double* dLU, int64_t lda, const 
 int lu_solve(lu_handle h, const double* dLU, int64_t lda, const int32_t* ipiv, double* dB, int64_t ldb,
              int64_t nrhs, int trans, void* stream) {
   LUB_TRY(check_common(h, dLU, lda));
+  if (h->cfg.layout == LU_LAYOUT_COL) return LU_ERR_UNSUPPORTED;
   if (!ipiv || !dB || nrhs < 1 || ldb < nrhs || (trans != 0 && trans != 1)) return LU_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   const int n = (int)h->cfg.n;
@@ -448,13 +462,20 @@ int lu_factor_solve(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double*
   if (!h || !db) return LU_ERR_ARG;
   if (h->cfg.precision != LU_PREC_FP64) return LU_ERR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
+  const bool col = h->cfg.layout == LU_LAYOUT_COL;
+  if (col) {
+    LUB_TRY(check_common(h, dA, lda));
+    LUB_TRY(launch_transpose_inplace(dA, lda, (int)h->cfg.n, s));
+  }
   LUB_TRY(factor_f64(h, dA, lda, ipiv, db, s));
-  return solve_permuted_f64(h, dA, lda, db, s);
+  LUB_TRY(solve_permuted_f64(h, dA, lda, db, s));
+  return col ? launch_transpose_inplace(dA, lda, (int)h->cfg.n, s) : LU_OK;
 }
 
 int lu_residual(lu_handle h, const double* dA, int64_t lda, const double* dx, const double* db,
                 lu_residual_info* out, void* stream) {
   if (!h || !dA || !dx || !db || !out || lda < h->cfg.n) return LU_ERR_ARG;
+  if (h->cfg.layout == LU_LAYOUT_COL) return LU_ERR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
   const int n = (int)h->cfg.n;
   LUB_TRY(launch_residual_f64(dA, lda, n, dx, db, nullptr, h->racc, s));
@@ -484,6 +505,7 @@ int lu_adjoint(lu_handle h, const double* dLU, int64_t lda, const int32_t* ipiv,
                const double* dW, int64_t ldw, int64_t nrhs, double* gradB, int64_t ldgb, double* gradA,
                int64_t ldga, void* stream) {
   LUB_TRY(check_common(h, dLU, lda));
+  if (h->cfg.layout == LU_LAYOUT_COL) return LU_ERR_UNSUPPORTED;
   const int64_t n = h->cfg.n;
   if (!ipiv || !dW || !gradB || nrhs < 1 || ldw < nrhs || ldgb < nrhs) return LU_ERR_ARG;
   if (gradA && (!dX || ldx < nrhs || ldga < n)) return LU_ERR_ARG;

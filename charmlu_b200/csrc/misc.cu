@@ -84,6 +84,32 @@ __global__ void __launch_bounds__(256) residual_f64_kernel(const double* A, int6
   }
 }
 
+// In-place transpose of the n x n matrix A (row pitch lda) by 32 x 32
+// tiles: the CTA of tile (bi, bj), bi <= bj, reads it and tile (bj, bi)
+// into shared memory and writes each back transposed into the other's
+// place (a diagonal tile is transposed in place). 32 x 8 threads.
+__global__ void __launch_bounds__(256) transpose_inplace_kernel(double* A, int64_t lda, int n) {
+  __shared__ double t1[32][33], t2[32][33];
+  const int bi = blockIdx.x, bj = blockIdx.y;
+  if (bi > bj) return;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int k = ty; k < 32; k += 8) {
+    int r = bi * 32 + k, c = bj * 32 + tx;
+    if (r < n && c < n) t1[k][tx] = A[(int64_t)r * lda + c];
+    r = bj * 32 + k;
+    c = bi * 32 + tx;
+    if (bi != bj && r < n && c < n) t2[k][tx] = A[(int64_t)r * lda + c];
+  }
+  __syncthreads();
+  for (int k = ty; k < 32; k += 8) {
+    int r = bj * 32 + k, c = bi * 32 + tx;  // tile (bj, bi) <- tile (bi, bj)^T
+    if (r < n && c < n) A[(int64_t)r * lda + c] = t1[tx][k];
+    r = bi * 32 + k;
+    c = bj * 32 + tx;  // tile (bi, bj) <- tile (bj, bi)^T
+    if (bi != bj && r < n && c < n) A[(int64_t)r * lda + c] = t2[tx][k];
+  }
+}
+
 // y[i] -= A[i, :] . x for i < m (one warp per row; k columns)
 __global__ void __launch_bounds__(256) gemv_sub_kernel(const double* A, int64_t lda, int m, int k, const double* x,
                                                        double* y) {
@@ -141,6 +167,15 @@ int launch_residual_f64(const double* A, int64_t lda, int n, const double* x, co
   LUB_CUDA(cudaMemsetAsync(acc, 0, sizeof(ResidualAccum), s));
   if (n <= 0) return LU_OK;
   residual_f64_kernel<<<ceil_div(n, 8), 256, 0, s>>>(A, lda, n, 0, n, x, b, r, acc);
+  LUB_LAUNCH_CHECK();
+  return LU_OK;
+}
+
+int launch_transpose_inplace(double* A, int64_t lda, int n, cudaStream_t s) {
+  if (n <= 1) return LU_OK;
+  const int nt = ceil_div(n, 32);
+  if (nt > 65535) return LU_ERR_UNSUPPORTED;
+  transpose_inplace_kernel<<<dim3(nt, nt), dim3(32, 8), 0, s>>>(A, lda, n);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }

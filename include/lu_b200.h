@@ -65,6 +65,15 @@ extern "C" {
                               update sums Lh*Uh + Lh*Ul + Ll*Uh on the tensor cores (near-FP32 factors) */
 
 /* ---- refinement mode --------------------------------------------------- */
+/* Storage of dA for lu_factor / lu_factor_solve.  LU_LAYOUT_COL
+ * (column-major, as LAPACK): the matrix is transposed in place, factored,
+ * and the factors transposed back, so dA ends with L\U column-major and the
+ * pivots are the same as for the row-major matrix.  Other entry points take
+ * row-major data; with LU_LAYOUT_COL they return LU_ERR_UNSUPPORTED
+ * (lu_transpose_square converts). */
+#define LU_LAYOUT_ROW  0
+#define LU_LAYOUT_COL  1
+
 #define LU_IR_CLASSIC  0   /* classical iterative refinement, GMRES-IR fallback on stagnation */
 #define LU_IR_GMRES    1   /* GMRES-IR from the start */
 
@@ -80,7 +89,7 @@ typedef struct lu_config {
   int32_t use_graph;       /* 1 = capture the schedule once per (n, b) as a CUDA graph and replay it */
   int32_t ir_mode;         /* LU_IR_* (mixed precision only) */
   int32_t ir_max_iter;     /* refinement iteration cap */
-  int32_t reserved;
+  int32_t layout;          /* LU_LAYOUT_ROW (default) or LU_LAYOUT_COL for lu_factor / lu_factor_solve */
   double  sing_threshold;  /* |u_jj| <= threshold sets info; the reference aborts at 100*eps (lu.ci:339) */
   double  ir_target;       /* refinement stops when r_hpl < ir_target (default 16) */
   int64_t spin_limit;      /* bounded-wait iteration cap for cross-CTA waits (0 = default) */
@@ -323,6 +332,12 @@ LU_API int lu_trsv_block(lu_handle h, const double* dT, int64_t ldt, int32_t w, 
  * (lu.ci:439-456). */
 LU_API int lu_gemv_update(lu_handle h, const double* dA, int64_t lda, int64_t m, int32_t k, const double* dx,
                           double* dy, void* stream);
+
+/* dA <- dA^T in place for an n x n FP64 matrix with row pitch lda (device;
+ * asynchronous on stream): converts between column- and row-major
+ * storage.  No reference counterpart (its blocks are row-major,
+ * lu.h:151-153). */
+LU_API int lu_transpose_square(double* dA, int64_t n, int64_t lda, void* stream);
 
 /* Copy a rows x width-byte block between host and device memory (either
  * direction; pitches in bytes), asynchronous on stream.  Host memory should

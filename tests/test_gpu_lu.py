@@ -274,3 +274,59 @@ def test_graph_replay_identical(cuda_dev, lookahead):
     A2 = torch.from_numpy(A).cuda()  # different buffer: re-capture
     p2 = g.factor(A2)
     assert g.status() == 0 and torch.equal(A2, Ar) and torch.equal(p2, pr)
+
+
+@pytest.mark.parametrize("n,b", [(1000, 128), (1001, 64), (2048, 256)])
+def test_column_major_layout_matches_row_major(cuda_dev, n, b):
+    """LU_LAYOUT_COL: a column-major A (LAPACK order) is transposed in place,
+    factored and transposed back, so its factors and pivots equal the
+    row-major factorisation's, bit for bit, stored column-major."""
+    lu = _lu()
+    A = torch.from_numpy(oracle.gen_matrix(n, 31)).cuda()
+    ld = n + (n & 1)
+    buf = torch.zeros(ld, ld, dtype=torch.float64, device="cuda")
+    buf[:n, :n] = A.t()
+    A_col = buf[:n, :n].t()  # column-major view of A: unit row stride, pitch ld
+    assert A_col.stride(0) == 1 and torch.equal(A_col, A)
+    s_col = lu.LUSolver(lu.LUConfig(n, b, layout=lu.LU_LAYOUT_COL))
+    ipiv_col = s_col.factor(A_col)
+    assert s_col.status() == 0
+    s_row = lu.LUSolver(lu.LUConfig(n, b))
+    ref = torch.zeros(n, ld, dtype=torch.float64, device="cuda")
+    ref[:, :n] = A
+    ipiv_row = s_row.factor(ref[:, :n])
+    assert torch.equal(ipiv_col, ipiv_row)
+    assert torch.equal(A_col, ref[:, :n])
+    # factor_solve on a fresh column-major copy gives the row-major path's x
+    buf[:n, :n] = A.t()
+    rhs = torch.from_numpy(oracle.gen_vector(n, 31)).cuda()
+    x_col = rhs.clone()
+    s_col.factor_solve(A_col, x_col)
+    ref[:, :n] = A
+    x_row = rhs.clone()
+    s_row.factor_solve(ref[:, :n], x_row)
+    assert torch.equal(x_col, x_row) and torch.equal(A_col, ref[:, :n])
+    # the other entry points take row-major data
+    with pytest.raises(lu.LUError) as e:
+        s_col.solve(A_col, ipiv_col, rhs.clone())
+    assert e.value.code == lu.LU_ERR_UNSUPPORTED
+
+
+def test_transpose_square_and_layout_arguments(cuda_dev):
+    lu = _lu()
+    for n in (1, 31, 32, 33, 1001):
+        ld = n + (n & 1) + 2
+        buf = torch.from_numpy(oracle.gen_uniform(n * ld, 5, 0).reshape(n, ld)).cuda()
+        A = buf[:, :n]
+        A0 = A.clone()
+        pad0 = buf[:, n:].clone()
+        lu.transpose_square(A)
+        torch.cuda.synchronize()
+        assert torch.equal(A, A0.t()) and torch.equal(buf[:, n:], pad0)
+        lu.transpose_square(A)
+        assert torch.equal(A, A0)
+    with pytest.raises(lu.LUError) as e:
+        lu.LUSolver(lu.LUConfig(256, 64, precision=lu.LU_PREC_FP16X3, layout=lu.LU_LAYOUT_COL))
+    assert e.value.code == lu.LU_ERR_UNSUPPORTED
+    with pytest.raises(lu.LUError):
+        lu.LUSolver(lu.LUConfig(256, 64, layout=7))
