@@ -24,7 +24,7 @@ EXPORTS = [
     "lu_profile", "lu_phase_times", "lu_launch_count", "lu_solve_noalloc",
     "lu_batched_work_bytes", "lu_batched_set_tuning", "lu_refine_factor", "lu_refine_apply",
     "lu_refine_adjoint", "lu_panel_factor", "lu_apply_pivots", "lu_trsm_lower_unit", "lu_gemm_update",
-    "lu_trsv_block", "lu_gemv_update", "lu_copy_2d", "lu_transpose_square",
+    "lu_trsv_block", "lu_gemv_update", "lu_copy_2d", "lu_transpose_square", "lu_status_clear",
 ]
 PHASES = ["panel", "laswp", "trsm", "gemm", "gemm_inner", "solve", "other"]
 
@@ -81,6 +81,7 @@ def load():
         "lu_gemv_update": ([H, P, i64, i64, i32, P, P, P], ctypes.c_int),
         "lu_copy_2d": ([P, i64, P, i64, i64, i64, P], ctypes.c_int),
         "lu_transpose_square": ([P, i64, i64, P], ctypes.c_int),
+        "lu_status_clear": ([H, P], ctypes.c_int),
         "lu_adjoint": ([H, P, i64, P, P, i64, P, i64, i64, P, i64, P, i64, P], ctypes.c_int),
         "lu_refine_factor": ([H, P, i64, P], ctypes.c_int),
         "lu_refine_apply": ([H, P, i64, i32, P, i64, P, i64, i64, ctypes.POINTER(LuRefineInfo), P], ctypes.c_int),

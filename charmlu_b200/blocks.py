@@ -83,6 +83,10 @@ class CudaBlocks:
         _check(self._L.lu_gemv_update(self._h, _ptr(A), A.stride(0), m, k, _ptr(x), _ptr(y), self._s()),
                "lu_gemv_update")
 
+    def clear_status(self):
+        """Clear the handle's status word before a factorisation."""
+        _check(self._L.lu_status_clear(self._h, self._s()), "lu_status_clear")
+
     def status(self):
         """First singular global column (1-based), a negative error code, or 0."""
         return int(self._L.lu_status(self._h, self._s()))

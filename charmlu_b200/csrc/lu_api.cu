@@ -384,6 +384,12 @@ int lu_status(lu_handle h, void* stream) {
   return st.info;
 }
 
+int lu_status_clear(lu_handle h, void* stream) {
+  if (!h) return LU_ERR_ARG;
+  LUB_CUDA(cudaMemsetAsync(h->st, 0, sizeof(DevStatus), (cudaStream_t)stream));
+  return LU_OK;
+}
+
 int lu_factor(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double* rhs, void* stream) {
   if (!h) return LU_ERR_ARG;
   if (h->cfg.precision != LU_PREC_FP64) return LU_ERR_UNSUPPORTED;

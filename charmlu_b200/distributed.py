@@ -140,6 +140,7 @@ class BlockCyclicLU:
         self.status_code holds the first singular column (1-based, lowest
         over ranks) or 0."""
         n, b, me = self.n, self.b, self.rank
+        self.blocks.clear_status()
         ipiv = torch.zeros(n, dtype=torch.int32, device=self.device)
         bufs = [torch.zeros(n * self.ldp + b, dtype=torch.float64, device=self.device) for _ in range(2)]
         if self.owner(0) == me:

@@ -55,9 +55,6 @@ class OutOfCoreLU:
             self.copy_stream = torch.cuda.Stream(device=self.device)
 
     # ---- copies and their ordering ---------------------------------------
-    def _new_event(self):
-        return torch.cuda.Event() if self.cuda else None
-
     def _copy(self, dst, src, after=None):
         """dst <- src on the copy stream after `after` (an event, or the
         main stream's work so far when None); returns an event the main
@@ -121,6 +118,7 @@ class OutOfCoreLU:
         n, w, bl = self.n, self.w, self.blocks
         nbp = (n + w - 1) // w
         dev = self.device
+        bl.clear_status()
         ipiv = torch.zeros(n, dtype=torch.int32, device=dev)
         P = torch.empty(n, self.ld, dtype=torch.float64, device=dev)
         bufs = [torch.empty(n, self.ld, dtype=torch.float64, device=dev) for _ in range(2)]

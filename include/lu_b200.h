@@ -136,6 +136,11 @@ LU_API size_t lu_workspace_bytes(const lu_config* cfg);
  * sequence on h: LU_OK, >0 singular column (1-based), or LU_ERR_*. */
 LU_API int lu_status(lu_handle h, void* stream);
 
+/* Clear the handle's device status word (asynchronous on stream).  The
+ * factor and refine entry points clear it themselves; callers of the
+ * per-block building blocks below clear it before each factorisation. */
+LU_API int lu_status_clear(lu_handle h, void* stream);
+
 /* FP64 LU with partial pivoting in place: P A = L U, L unit lower.
  * Replaces LUBlk::factor() (lu.ci:31-42) and its kernels (lu.C:26-352).
  *   dA   : n x n row-major, lda >= n, overwritten with L\U

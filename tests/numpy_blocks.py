@@ -55,5 +55,8 @@ class NumpyBlocks:
     def gemv_update(self, A, x, y):
         y.numpy()[:] -= A.numpy() @ x.numpy()
 
+    def clear_status(self):
+        self.first_singular = 0
+
     def status(self):
         return self.first_singular

@@ -48,3 +48,17 @@ def test_panel_width_from_device_budget():
     # three n x w FP64 panels within the budget, w a multiple of b
     assert ooc.w % 256 == 0 and 3 * 8 * 131072 * ooc.w <= 90 << 30
     assert OutOfCoreLU(1000, b=256, blocks=NumpyBlocks(), device="cpu", device_budget=1 << 20).w == 256
+
+
+def test_status_is_cleared_between_factorisations():
+    """A driver reused after a singular matrix reports 0 for a regular one."""
+    from charmlu_b200.ooc import OutOfCoreLU
+    n = 64
+    ooc = OutOfCoreLU(n, panel=16, blocks=NumpyBlocks(), device="cpu")
+    A = np.random.default_rng(2).uniform(-0.5, 0.5, (n, n))
+    S = A.copy()
+    S[:, 5] = 0.0
+    ooc.factor(torch.from_numpy(S))
+    assert ooc.status_code == 6
+    ooc.factor(torch.from_numpy(A.copy()))
+    assert ooc.status_code == 0
