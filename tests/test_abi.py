@@ -74,3 +74,27 @@ def test_product_does_not_import_oracle():
                 txt = open(os.path.join(dirpath, f)).read()
                 assert "import oracle" not in txt and "from oracle" not in txt, f
                 assert "liboracle" not in txt, f
+
+
+def _header_param_counts():
+    """Parameter count of every LU_API declaration in include/lu_b200.h."""
+    txt = open(os.path.join(ROOT, "include", "lu_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    out = {}
+    for m in re.finditer(r"LU_API\s+(?:int|int64_t|size_t|const char\*)\s+(lu_\w+)\s*\(([^)]*)\)", txt):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_bindings_match_header_parameter_counts():
+    """The ctypes signature table declares as many arguments as the header
+    does for every entry point (an ABI change without its binding fails
+    here, on CPU)."""
+    from charmlu_b200 import _lib
+    L = _lib.load()
+    counts = _header_param_counts()
+    assert set(counts) == set(_lib.EXPORTS)
+    for name, k in counts.items():
+        argtypes = getattr(L, name).argtypes
+        assert argtypes is not None and len(argtypes) == k, (name, k, argtypes)
