@@ -863,6 +863,17 @@ def main():
                 "achieved": gemm_tf, "peak": peak_v, "unit": "TFLOP/s",
                 "frac": (gemm_tf / peak_v) if gemm_tf else None, "traffic": None,
                 "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"}
+        if args.lookahead and gemm_tf:
+            # beside the look-ahead panel the rest of each update runs on the
+            # SMs the panel's reserve leaves it: its fraction of those SMs' peak
+            try:
+                sms = torch.cuda.get_device_properties(dev).multi_processor_count
+                held = sms - int(os.environ.get("LU_B200_GEMM_RESERVE", "48"))
+                if 0 < held < sms:
+                    roof["sms_held"] = held
+                    roof["frac_of_sms_held"] = gemm_tf / (peak_v * held / sms)
+            except Exception:
+                pass
         tpath = os.path.join(ROOT, "profiles", "gemm_lowp_persistent_traffic.json")
     else:
         roof = {"bound": "tensor", "kernel": "gemm_f64_sub_kernel (trailing update, DMMA)",
