@@ -1,8 +1,10 @@
 """The out-of-core FP64 LU (charmlu_b200/ooc.py) on the GPU: the matrix in
-pinned host memory, column panels streamed through the device. Pivots equal
-lu_factor's (the same partial-pivoting choices on the same matrix), the
-factors agree to rounding (left-looking accumulates the updates in another
-order), and the streamed solve meets the HPL residual bar."""
+pinned host memory, column panels streamed through the device. The host
+factors satisfy P A = L U to rounding, the streamed solve meets the HPL
+residual bar and agrees with lu_factor's solution, and where the pivot
+sequences agree (they do unless two candidates tie to rounding; the
+left-looking order accumulates updates differently) the factors agree with
+lu_factor's to rounding."""
 import pytest
 import torch
 
