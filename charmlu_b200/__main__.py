@@ -6,7 +6,10 @@
 
 Same positional arguments as charmlu (benchmark.C:81-134); the memory
 threshold, mapping scheme and PE-tile arguments configure Charm++ placement
-and are accepted and ignored on one GPU.  Prints the reference's result
+and are accepted and ignored.  Under torchrun with several processes (one
+per GPU, as charmrun +pN gives the reference N PEs) the FP64 solve runs on
+the 1D block-cyclic driver over NCCL (charmlu_b200.distributed) and rank 0
+prints the result lines.  Prints the reference's result
 lines (benchmark.C:151-184, 352-356, 394-395), including the
 ``residual = %f`` line that test_lu.pl parses (test_lu.pl:76-77).  A is the
 counter-based uniform[-0.5,0.5) matrix; b is the reference's MatGen stream
@@ -14,8 +17,74 @@ counter-based uniform[-0.5,0.5) matrix; b is the reference's MatGen stream
 """
 import argparse
 import json
+import os
 import sys
 import time
+
+
+def _header(n, b, batch, mem, mapping, procs):
+    print("Running LU compiled from revision: charmlu_b200")
+    print(f"Running LU on {procs} processors (1 nodes): \n\tMatrix size: {n} X {n} \n\tBlock size: {b} X {b} "
+          f"\n\tChare Array size: {n // b} X {n // b}\n\tPivot batch size: {batch}\n\tMem Threshold (MB): {mem}"
+          f"\n\tSend Limit: 0\n\tMapping Scheme: {mapping} ({'Block Cyclic' if mapping == 2 else '2D Tiling'})")
+
+
+def _report(n, b, procs, dt, st, r, eps):
+    if st > 0:
+        print("Diagonal element very small despite pivoting. Is the matrix singular??")
+    gflops = (2.0 / 3.0 * n ** 3 + 1.5 * n ** 2) / dt / 1e9
+    print(f"RESULT procs: \t{procs}\tblock size:\t{b}\tTime(s):\t{dt}")
+    print(f"HPL flop count gives \t{gflops}\tGFlops")
+    print(f"epsilon = {eps:e}\nresidual = {r['r_ref']:f}")
+    if r["r_ref"] > 16:
+        print("=== WARNING: Scaled residual is greater than 16 - OUT OF SPEC ===")
+    print(f"r_hpl = {r['r_hpl']:f}")
+    return gflops
+
+
+def _main_ranks(n, b, mem, batch, mapping, a, world):
+    """The FP64 solve over `world` GPUs, one process each (torchrun)."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    import charmlu_b200 as lu
+    from charmlu_b200.distributed import BlockCyclicLU
+    if a.precision != "fp64":
+        print("Only the FP64 solve runs over several GPUs; run one process for --precision", a.precision)
+        return 1
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group("nccl", device_id=dev, timeout=datetime.timedelta(seconds=600))
+    try:
+        if rank == 0:
+            _header(n, b, batch, mem, mapping, world)
+        d = BlockCyclicLU(n, b, lookahead=True)
+        A = lu.generate_uniform(n, n, seed=a.seed, stream_id=0, device=dev)
+        loc = d.scatter(A)
+        bvec = torch.from_numpy(lu.matgen(n)).to(dev)
+        if rank == 0:
+            print("Starting solve")
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ipiv = d.factor(loc)
+        x = d.solve(loc, ipiv, bvec)
+        torch.cuda.synchronize()
+        dist.barrier()
+        dt = time.perf_counter() - t0
+        if rank == 0:
+            r = lu.LUSolver(lu.LUConfig(n, b)).residual(A, x, bvec)
+            gflops = _report(n, b, world, dt, d.status_code, r, lu.EPS)
+            if a.json:
+                print(json.dumps({"n": n, "b": b, "precision": "fp64", "procs": world, "time_s": dt,
+                                  "gflops_ref_count": gflops, "status": d.status_code, **r}))
+            print("Finished solve")
+    finally:
+        dist.destroy_process_group()
+    return 0
 
 
 def main(argv=None):
@@ -41,14 +110,15 @@ def main(argv=None):
         print(f"The matrix size {n} should be a multiple of block size {b}!")
         return 0
 
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        return _main_ranks(n, b, mem, batch, mapping, a, world)
+
     import torch
     import charmlu_b200 as lu
     prec = {"fp64": lu.LU_PREC_FP64, "bf16": lu.LU_PREC_BF16, "fp16s": lu.LU_PREC_FP16S,
             "fp16x3": lu.LU_PREC_FP16X3}[a.precision]
-    print("Running LU compiled from revision: charmlu_b200")
-    print(f"Running LU on 1 processors (1 nodes): \n\tMatrix size: {n} X {n} \n\tBlock size: {b} X {b} "
-          f"\n\tChare Array size: {n // b} X {n // b}\n\tPivot batch size: {batch}\n\tMem Threshold (MB): {mem}"
-          f"\n\tSend Limit: 0\n\tMapping Scheme: {mapping} ({'Block Cyclic' if mapping == 2 else '2D Tiling'})")
+    _header(n, b, batch, mem, mapping, 1)
     A = lu.generate_uniform(n, n, seed=a.seed, stream_id=0)
     bvec = torch.from_numpy(lu.matgen(n)).cuda()
     A0 = A.clone()
@@ -66,16 +136,8 @@ def main(argv=None):
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     st = s.status()
-    if st > 0:
-        print("Diagonal element very small despite pivoting. Is the matrix singular??")
-    gflops = (2.0 / 3.0 * n ** 3 + 1.5 * n ** 2) / dt / 1e9
-    print(f"RESULT procs: \t1\tblock size:\t{b}\tTime(s):\t{dt}")
-    print(f"HPL flop count gives \t{gflops}\tGFlops")
     r = s.residual(A0, x, bvec)
-    print(f"epsilon = {lu.EPS:e}\nresidual = {r['r_ref']:f}")
-    if r["r_ref"] > 16:
-        print("=== WARNING: Scaled residual is greater than 16 - OUT OF SPEC ===")
-    print(f"r_hpl = {r['r_hpl']:f}")
+    gflops = _report(n, b, 1, dt, st, r, lu.EPS)
     if a.json:
         print(json.dumps({"n": n, "b": b, "precision": a.precision, "time_s": dt, "gflops_ref_count": gflops,
                           "tflops": (2 / 3 * n ** 3 + 2 * n ** 2) / dt / 1e12, "status": st, "refine": info, **r}))
