@@ -1,10 +1,11 @@
 // lu_solve_noalloc: the solve of lu_solve (one right-hand side, trans = 0)
 // for callers that cannot allocate device memory.
 //
-// Who needs it: code that runs where cudaMalloc is not allowed or not
-// wanted — inside a region being captured into a CUDA graph, from a
-// real-time or plugin host that hands the library a fixed memory budget up
-// front, or from a caller that has no solver handle (lu_create allocates the
+// Who needs it: callers that may not allocate device memory.  A plugin
+// inside a host application that owns all device memory through its own
+// allocator and hands the library a fixed budget up front; a real-time loop
+// that cannot afford cudaMalloc/cudaFree, which may synchronise the whole
+// device; and a caller that has no solver handle (lu_create allocates the
 // handle's workspace).  This entry point allocates nothing: its only scratch
 // (the substitution pipeline's ready flags, its ticket counter and a status
 // word) lives in the file-scope device array below, which every GPU that
@@ -14,7 +15,10 @@
 //
 // Set-up: the first call on each device looks up the array's device address
 // with cudaGetSymbolAddress (with that device current) and caches it; make
-// that first call before any stream capture.  Host code must not hand the
+// that first call before any stream capture.  The cached address belongs to
+// the device's context at that time: after cudaDeviceReset (or any other end
+// of the primary context) it is stale, so a process that resets a device
+// must not call this entry point on it again.  Host code must not hand the
 // array's name to a kernel: on the host it is only a stand-in, not a device
 // address.
 //

@@ -158,7 +158,7 @@ def test_exact_tie_lowest_row_wins(cuda_dev, lookahead):
     oracle (lowest global row wins an exact tie)."""
     A = oracle.gen_matrix(4096, 3)
     A[10, 0], A[1000, 0], A[3000, 0] = -1.0, 1.0, -1.0
-    _, _, ipiv_ref, _, _ = oracle.lu_factor(A, b=256)
+    _, ipiv_ref, _, _, _ = oracle.lu_factor(A, b=256)
     s, Ag, ipiv, _, st = _gpu_factor(A, 256, lookahead=lookahead)
     assert st == 0 and int(ipiv[0]) == 10 and ipiv_ref[0] == 10
 
@@ -330,3 +330,19 @@ def test_transpose_square_and_layout_arguments(cuda_dev):
     assert e.value.code == lu.LU_ERR_UNSUPPORTED
     with pytest.raises(lu.LUError):
         lu.LUSolver(lu.LUConfig(256, 64, layout=7))
+    # a rejected argument leaves a column-major matrix untouched (the in-place
+    # transpose runs only after every check has passed)
+    import ctypes
+    from charmlu_b200 import _lib
+    n = 256
+    s_col = lu.LUSolver(lu.LUConfig(n, 64, layout=lu.LU_LAYOUT_COL))
+    A = torch.from_numpy(oracle.gen_matrix(n, 9)).cuda()
+    A0 = A.clone()
+    x = torch.ones(n, dtype=torch.float64, device="cuda")
+    L = _lib.load()
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert L.lu_factor(s_col._h, ctypes.c_void_p(A.data_ptr()), n, None, None, st) == lu.LU_ERR_ARG
+    assert L.lu_factor_solve(s_col._h, ctypes.c_void_p(A.data_ptr()), n, None,
+                             ctypes.c_void_p(x.data_ptr()), st) == lu.LU_ERR_ARG
+    torch.cuda.synchronize()
+    assert torch.equal(A, A0)

@@ -1,9 +1,10 @@
 """lu_solve_noalloc: the allocation-free solve, checked against lu_solve.
 
-Some callers cannot allocate device memory (inside a CUDA graph capture, on
-a host with a fixed device-memory budget, or without a solver handle, whose
-creation allocates).  lu_solve_noalloc serves them with its scratch in a
-fixed device array inside the library.  This file is collected last so a
+Some callers may not allocate device memory: a plugin whose host
+application owns the device memory and grants it a fixed budget, a real-time
+loop that cannot afford an allocation's device-wide synchronisation, or a
+caller without a solver handle (creating one allocates).  lu_solve_noalloc
+serves them with its scratch in a fixed device array inside the library.  This file is collected last so a
 run that stops at the first failure has run every other test first; each
 test also passes alone in a fresh process.
 """
