@@ -28,6 +28,36 @@ TEST_LU_PL_ARGS = [
 RESIDUAL = re.compile(r"residual = ([\d\.]*)")  # test_lu.pl:77
 
 
+# every line the reference prints around a solve (benchmark.C:150-184, 343-400)
+FLOAT = r"[-+]?(?:\d+\.?\d*(?:[eE][-+]?\d+)?|inf|nan)"
+REF_LINES = [
+    r"^Running LU compiled from revision: \S+$",
+    r"^Running LU on \d+ processors \(\d+ nodes\): $",
+    r"^\tMatrix size: \d+ X \d+ $",
+    r"^\tBlock size: \d+ X \d+ $",
+    r"^\tChare Array size: \d+ X \d+$",
+    r"^\tPivot batch size: \d+$",
+    r"^\tMem Threshold \(MB\): \d+$",
+    r"^\tSend Limit: \d+$",
+    r"^\tMapping Scheme: \d+ \((Block Cyclic|2D Tiling)\)$",
+    r"^\tPivot Redn Scheduling: (On|Off)$",
+    r"^\tUseg Multicast from: (Below|Diagonal)$",
+    r"^RESULT procs: \t\d+\tblock size:\t\d+\tTime\(s\):\t" + FLOAT + "$",
+    r"^HPL flop count gives \t" + FLOAT + r"\tGFlops$",
+    r"^Order:\t" + FLOAT + "% of peak$",
+    r"^Abe:\t" + FLOAT + "% of peak$",
+    r"^Ranger:\t" + FLOAT + "% of peak$",
+    r"^Jaguar/Kraken XT5:\t" + FLOAT + "% of peak$",
+    r"^BG/P:\t" + FLOAT + "% of peak$",
+    r"^Jaguar XK6 sans GPUs:\t" + FLOAT + "% of peak$",
+    r"^The dgemm \d+ x \d+ takes " + FLOAT + " ms and achieves " + FLOAT + " GFlop/sec$",
+    r"^Percent of DGEMM is: " + FLOAT + "%$",
+    r"^epsilon = \d\.\d{6}e[-+]\d+$",
+    r"^residual = \d+\.\d{6}$",
+    r"^finished validation at wall time: \d+\.\d{6}$",
+]
+
+
 @pytest.mark.parametrize("args", TEST_LU_PL_ARGS, ids=lambda a: "_".join(map(str, a)))
 def test_cli_residual_line(cuda_dev, capsys, args):
     from charmlu_b200.__main__ import main
@@ -38,6 +68,26 @@ def test_cli_residual_line(cuda_dev, capsys, args):
     assert float(m.group(1)) < 16, out
     assert "RESULT procs:" in out and "HPL flop count gives" in out
     assert f"Pivot batch size: {args[3] if len(args) > 3 else args[1] // 4}" in out
+
+
+@pytest.mark.parametrize("args", [[512, 128, 500], [512, 64, 500, 128, 3, 4, 1, 2]],
+                         ids=lambda a: "_".join(map(str, a)))
+def test_cli_prints_every_reference_line(cuda_dev, capsys, args):
+    """Each result and configuration line of the reference has its
+    counterpart, in the reference's format, in the reference's order."""
+    from charmlu_b200.__main__ import main
+    assert main([str(v) for v in args]) in (0, None)
+    lines = capsys.readouterr().out.splitlines()
+    pos = -1
+    for pat in REF_LINES:
+        hits = [i for i, ln in enumerate(lines) if re.match(pat, ln)]
+        assert hits, (pat, lines)
+        assert hits[0] > pos, (pat, lines)
+        pos = hits[0]
+    if len(args) >= 5 and args[4] == 3:
+        assert f"\tMapping PE tile size: {args[5]} x {args[6]} rotate {args[7]} stride {args[6]} " in lines
+    dg = [ln for ln in lines if ln.startswith("The dgemm")][0]
+    assert f"The dgemm {args[1]} x {args[1]} takes" in dg and float(dg.split()[-2]) > 0
 
 
 def test_cli_process_entry_point(cuda_dev):
