@@ -6,9 +6,9 @@ Each building block is checked against a plain FP64 torch / scipy
 reference of the same operation. The driver at world size 1 (NCCL, one
 rank) runs the same kernels on the same shapes as lu_factor, so without
 look-ahead its factors and pivots equal lu_factor's bit for bit; with
-look-ahead the pivots are equal and the factors agree to rounding. Several
-ranks are covered on CPU (tests/test_distributed_lu.py): this pool gives
-one GPU per run."""
+look-ahead the pivots are equal and the factors agree to rounding. World
+sizes above one are covered on CPU with gloo ranks (tests/test_distributed_lu.py,
+tests/test_distributed_2d.py)."""
 import os
 
 import numpy as np
@@ -173,3 +173,27 @@ def test_block_cyclic_one_rank_singular(cuda_dev, one_rank_group):
     d = BlockCyclicLU(n, b)
     d.factor(d.scatter(A))
     assert d.status_code == 301
+
+
+@pytest.mark.parametrize("n,b", [(1000, 128), (2048, 256)])
+def test_block_cyclic_2d_one_rank_matches_lu_factor(cuda_dev, one_rank_group, n, b):
+    """The 2D driver on a 1 x 1 grid: its panel gather, interchange exchange
+    and U broadcast reduce to local copies, so it runs lu_factor's kernels
+    on the same blocks: the same pivots, the factors equal to rounding."""
+    import charmlu_b200 as lu
+    from charmlu_b200.distributed import BlockCyclic2DLU
+    A = lu.generate_uniform(n, n, seed=19, stream_id=0)
+    rhs = lu.generate_uniform(n, 1, seed=19, stream_id=1).view(-1)
+    d = BlockCyclic2DLU(n, b, 1, 1)
+    loc = d.scatter(A)
+    ipiv = d.factor(loc)
+    assert d.status_code == 0
+    x = d.solve(loc, ipiv, rhs)
+    s = lu.LUSolver(lu.LUConfig(n, b))
+    ref = A.clone()
+    ipiv_ref = s.factor(ref)
+    assert torch.equal(ipiv, ipiv_ref)
+    LU = d.gather(loc)
+    assert (LU - ref).abs().max().item() <= 1e-12 * ref.abs().max().item() * n
+    r = s.residual(A, x, rhs)
+    assert r["r_hpl"] < 16, r
