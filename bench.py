@@ -118,6 +118,56 @@ def cpu_baseline(n_sample=8192, b=256, reps=2):
                       f"r_hpl={res['r_hpl']:.3g}; the N=65536 step would take ~{flops_lu(65536) / (flops_lu(n_sample) / best) / 60:.0f} min on these cores"}
 
 
+def fp64_c2_record(dev, peak64, steps=3, with_cpu=True):
+    """The FP64 path at N=32768, b=256 (factor + solve with look-ahead,
+    inputs resident in HBM, 8.6 GB > L2), timed with CUDA events, beside the
+    CPU oracle at the same order run once on all host cores."""
+    import torch
+    import charmlu_b200 as lu
+    n, b = 32768, 256
+    A0 = lu.generate_uniform(n, n, seed=42, stream_id=0, device=dev)
+    rhs0 = lu.generate_uniform(n, 1, seed=42, stream_id=1, device=dev).view(-1)
+    A = torch.empty_like(A0)
+    x = torch.empty_like(rhs0)
+    s = lu.LUSolver(lu.LUConfig(n, b, lookahead=True))
+    ms = []
+    for k in range(1 + steps):
+        A.copy_(A0)
+        x.copy_(rhs0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s.factor_solve(A, x)
+        e1.record()
+        torch.cuda.synchronize()
+        if k:
+            ms.append(e0.elapsed_time(e1))
+    st = s.status()
+    r = s.residual(A0, x, rhs0)
+    t = sum(ms) / len(ms) / 1e3
+    rec = {"n": n, "block_size": b, "lookahead": True, "steps": steps, "time_s": t,
+           "tflops": flops_lu(n) / t / 1e12, "frac_of_fp64_peak": flops_lu(n) / t / 1e12 / peak64,
+           "status": st, "r_hpl": r["r_hpl"], "r_ref": r["r_ref"]}
+    x_gpu = x.cpu().numpy()
+    del A0, A, x, rhs0
+    s.close()
+    torch.cuda.empty_cache()
+    if with_cpu:
+        import oracle
+        cores = os.cpu_count() or 1
+        oracle.set_threads(cores)
+        Ah = oracle.gen_matrix(n, 42)
+        bh = oracle.gen_uniform(n, 42, 1)
+        t0 = time.perf_counter()
+        xc, *_ = oracle.solve(Ah, bh, b=b)
+        tc = time.perf_counter() - t0
+        rc = oracle.residual(Ah, xc, bh)
+        rec["cpu_same_n"] = {"kind": "port", "cores": cores, "time_s": tc, "tflops": flops_lu(n) / tc / 1e12,
+                             "r_hpl": rc["r_hpl"], "gpu_speedup": tc / t,
+                             "x_rel_diff_gpu_vs_cpu": float(abs(x_gpu - xc).max() / abs(xc).max()),
+                             "sample": f"N={n} b={b} factor+solve, one run (the oracle restatement of charmlu)"}
+    return rec
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -154,28 +204,16 @@ def run_reference(args, rank, world):
     return 0
 
 
-def run_batched(args, rank, world):
-    """4096 independent systems, orders log-uniform in [32, 1024] (seed 42),
-    one RHS each, factored and solved in one persistent launch replayed from
-    a CUDA graph; FP64 and FP32-factor + FP64-refinement; against a loop of
-    the single-matrix path on the same GPU.  With N > 1 GPUs the one set of
-    systems is split by cost (partition_by_cost): no collective but a final
-    gather of per-system status and scaled residual; time = max over ranks
-    (strong scaling: total work fixed)."""
+def batched_measure(n_all, mine, dev, dist, steps, warmup, world=1):
+    """Time the batched solver on this rank's systems (indices `mine` of the
+    orders n_all): one persistent launch, captured in a CUDA graph and
+    replayed, in FP64 and in FP32 with FP64 refinement.  Returns per mode the
+    mean replay time (max over ranks), throughput on all systems, failures
+    and the largest per-system scaled residual, plus the buffers."""
     import numpy as np
     import torch
     import charmlu_b200 as lu
-    from charmlu_b200.batched import BatchedSystems, flops, gather_results, log_uniform_orders, partition_by_cost
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", device_id=dev, timeout=datetime.timedelta(seconds=300))
-    n_all = log_uniform_orders(args.batch_count, 32, 1024, seed=42)
-    mine = partition_by_cost(n_all, world)[rank]
+    from charmlu_b200.batched import BatchedSystems, flops, gather_results, partition_by_cost
     n = n_all[mine]
     # the global data set (counter-based generator), this rank's systems copied out
     g = BatchedSystems(n_all, device=dev)
@@ -201,7 +239,7 @@ def run_batched(args, rank, world):
         with torch.cuda.graph(graph):
             bs.factor_solve(A, b, prec)
         ms = []
-        for k in range(args.warmup + args.steps):
+        for k in range(warmup + steps):
             A.copy_(A0)
             b.copy_(b0)
             torch.cuda.synchronize()
@@ -215,7 +253,7 @@ def run_batched(args, rank, world):
             t = torch.tensor([e0.elapsed_time(e1)], device=dev)
             if dist:
                 dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            if k >= args.warmup:
+            if k >= warmup:
                 ms.append(float(t))
         # every system's scaled residual against the untouched FP64 data
         res = np.empty(len(n))
@@ -232,7 +270,41 @@ def run_batched(args, rank, world):
         out[name] = {"ms": t, "tflops": F_all / (t / 1e3) / 1e12, "systems_per_s": len(n_all) / (t / 1e3),
                      "bad_systems": int((g_info != 0).sum()), "r_hpl_max": float(np.nanmax(g_res)),
                      "systems_per_rank": [int(len(p)) for p in partition_by_cost(n_all, world)]}
+        if prec == lu.LU_PREC_FP32:
+            # systems that met r_hpl < 16 after 0, 1, 2, ... FP64 refinement
+            # steps (this rank's share), the last entry not at all
+            hist = bs.refine_histogram().tolist()
+            out[name]["refine_steps_histogram"] = hist
+            out[name]["systems_needing_more_than_one_step"] = int(sum(hist[2:]))
         del graph
+    return out, bs, A, b, A0, b0
+
+
+def run_batched(args, rank, world):
+    """4096 independent systems, orders log-uniform in [32, 1024] (seed 42),
+    one RHS each, factored and solved in one persistent launch replayed from
+    a CUDA graph; FP64 and FP32-factor + FP64-refinement; against a loop of
+    the single-matrix path on the same GPU.  With N > 1 GPUs the one set of
+    systems is split by cost (partition_by_cost): no collective but a final
+    gather of per-system status and scaled residual; time = max over ranks
+    (strong scaling: total work fixed)."""
+    import numpy as np
+    import torch
+    import charmlu_b200 as lu
+    from charmlu_b200.batched import BatchedSystems, flops, gather_results, log_uniform_orders, partition_by_cost
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", device_id=dev, timeout=datetime.timedelta(seconds=300))
+    n_all = log_uniform_orders(args.batch_count, 32, 1024, seed=42)
+    mine = partition_by_cost(n_all, world)[rank]
+    out, bs, A, b, A0, b0 = batched_measure(n_all, mine, dev, dist, args.steps, args.warmup, world)
+    n = n_all[mine]
+    F_all = flops(n_all)
     loop_ms = None
     if world == 1:
         # a loop of the single-matrix path (one handle per distinct order, created before timing)
@@ -674,6 +746,8 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=8192)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-c2", action="store_true")        # skip the N=32768 FP64 sub-record
+    ap.add_argument("--no-batched", action="store_true")   # skip the batched sub-record
     ap.add_argument("--workload", default="lu", choices=["lu", "batched", "ksweep", "adjoint", "ooc",
                                                          "blockcyclic", "ooc64"])
     ap.add_argument("--ooc-n", type=int, default=65536)
@@ -856,13 +930,22 @@ def main():
     gms, gcalls, gfl = phases["gemm"]
     gemm_tf = gfl / gms / 1e9 if gms > 0 else None
     if mode == "mixed":
-        peak_v = peaks.get("bf16_tflops_sustained") or 1376.1
+        peak_v, peak_src = (peaks.get("bf16_tflops_sustained"), "MEASURED_PEAKS.json bf16_tflops_sustained "
+                                                                "(of measured)")
+        if not peak_v:
+            peak_v, peak_src = 1400.0, "fallback sustained bf16 figure (MEASURED_PEAKS.json absent; of fallback)"
+        # the phase counts executed tensor flops: three FP16 products per
+        # element for the error-compensated split, one otherwise
+        prods = 3 if args.precision == "fp16x3" else 1
+        alg_tf = gemm_tf / prods if gemm_tf else None
         roof = {"bound": "tensor", "kernel": f"gemm_lowp_persistent_kernel (trailing update, tcgen05 kind::f16 "
-                                             f"{args.precision}, double-buffered TMEM accumulators; flops counted "
-                                             "as executed, 3x for fp16x3)",
-                "achieved": gemm_tf, "peak": peak_v, "unit": "TFLOP/s",
-                "frac": (gemm_tf / peak_v) if gemm_tf else None, "traffic": None,
-                "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"}
+                                             f"{args.precision}, double-buffered TMEM accumulators)",
+                "achieved": alg_tf, "peak": peak_v, "unit": "TFLOP/s",
+                "frac": (alg_tf / peak_v) if alg_tf else None, "traffic": None,
+                "flops_counted": "algorithmic: 2*M*N*K per trailing update, each product once",
+                "achieved_executed": gemm_tf, "frac_executed": (gemm_tf / peak_v) if gemm_tf else None,
+                "executed_note": f"{prods} tensor-core product(s) per element ({args.precision})",
+                "peak_source": peak_src}
         if args.lookahead and gemm_tf:
             # beside the look-ahead panel the rest of each update runs on the
             # SMs the panel's reserve leaves it: its fraction of those SMs' peak
@@ -871,7 +954,7 @@ def main():
                 held = sms - int(os.environ.get("LU_B200_GEMM_RESERVE", "48"))
                 if 0 < held < sms:
                     roof["sms_held"] = held
-                    roof["frac_of_sms_held"] = gemm_tf / (peak_v * held / sms)
+                    roof["frac_executed_of_sms_held"] = gemm_tf / (peak_v * held / sms)
             except Exception:
                 pass
         tpath = os.path.join(ROOT, "profiles", "gemm_lowp_persistent_traffic.json")
@@ -957,6 +1040,18 @@ def main():
             line["e2e"] = {"value": None, "unit": "TFLOP/s", "h2d_bytes_per_step": 8 * n * n + 8 * n,
                            "d2h_bytes_per_step": 8 * n,
                            "note": f"host RAM available {avail / 1e9:.0f} GB < {need / 1e9:.0f} GB needed for pinned A"}
+    if rank == 0 and world == 1 and not args.no_c2:
+        # the BASELINE's N=32768 FP64 configuration, with the CPU oracle at the same order
+        line["fp64_c2"] = fp64_c2_record(dev, peak64_v, with_cpu=not args.no_cpu)
+    if rank == 0 and world == 1 and not args.no_batched:
+        from charmlu_b200.batched import log_uniform_orders
+        import numpy as np
+        n_all = log_uniform_orders(args.batch_count, 32, 1024, seed=42)
+        bout = batched_measure(n_all, np.arange(len(n_all)), dev, None, 3, 3)[0]
+        line["batched"] = {"workload": f"{len(n_all)} systems, n log-uniform [32,1024] seed 42, one RHS each, "
+                                       "one persistent launch replayed from a CUDA graph",
+                           "fp64": bout["fp64"], "fp32_ir": bout["fp32_ir"]}
+        torch.cuda.empty_cache()
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline()
     if rank == 0:

@@ -75,6 +75,9 @@ class LUConfig:
     sing_threshold: float = 0.0        # reference: 100*eps aborts (lu.ci:339)
     spin_limit: int = 0
     layout: int = LU_LAYOUT_ROW        # LU_LAYOUT_COL: factor / factor_solve take column-major A
+    gmres_restart: int = 0             # GMRES-IR Krylov vectors per cycle (0: 120)
+    ir_stall: int = 0                  # GMRES cycles in a row with < 10% residual drop before giving up (0: 3)
+    gmres_tol: float = 0.0             # residual reduction that ends a GMRES cycle (0: 1e-10)
 
     def to_c(self):
         c = _lib.LuConfig()
@@ -91,6 +94,9 @@ class LUConfig:
         c.sing_threshold = float(self.sing_threshold)
         c.spin_limit = int(self.spin_limit)
         c.layout = int(self.layout)
+        c.gmres_restart = int(self.gmres_restart)
+        c.ir_stall = int(self.ir_stall)
+        c.gmres_tol = float(self.gmres_tol)
         return c
 
 
@@ -262,6 +268,16 @@ class LUSolver:
         refine_apply / refine_adjoint (lu_refine_factor; A untouched)."""
         lda = self._check_matrix(A)
         _check(self._L.lu_refine_factor(self._h, _ptr(A), lda, _stream(stream)), "lu_refine_factor")
+
+    def refine_precond_norm(self, A, iters=10, stream=None):
+        """Power-iteration estimate of ||I - M^{-1} A|| for the factors M kept
+        by refine_factor (lu_refine_precond_norm): classical refinement
+        contracts by about this factor per step."""
+        lda = self._check_matrix(A)
+        est = ctypes.c_double(0.0)
+        _check(self._L.lu_refine_precond_norm(self._h, _ptr(A), lda, int(iters), ctypes.byref(est),
+                                              _stream(stream)), "lu_refine_precond_norm")
+        return est.value
 
     def refine_apply(self, A, B, X=None, trans=False, stream=None):
         """op(A) X = B (op = A^T with trans) by FP64 iterative refinement on

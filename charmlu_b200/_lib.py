@@ -25,6 +25,7 @@ EXPORTS = [
     "lu_batched_work_bytes", "lu_batched_set_tuning", "lu_refine_factor", "lu_refine_apply",
     "lu_refine_adjoint", "lu_panel_factor", "lu_apply_pivots", "lu_trsm_lower_unit", "lu_gemm_update",
     "lu_trsv_block", "lu_gemv_update", "lu_copy_2d", "lu_transpose_square", "lu_status_clear",
+    "lu_refine_precond_norm", "lu_batched_refine_histogram",
 ]
 PHASES = ["panel", "laswp", "trsm", "gemm", "gemm_inner", "solve", "other"]
 
@@ -35,6 +36,7 @@ class LuConfig(ctypes.Structure):
         ("precision", ctypes.c_int32), ("lookahead", ctypes.c_int32), ("use_graph", ctypes.c_int32),
         ("ir_mode", ctypes.c_int32), ("ir_max_iter", ctypes.c_int32), ("layout", ctypes.c_int32),
         ("sing_threshold", ctypes.c_double), ("ir_target", ctypes.c_double), ("spin_limit", ctypes.c_int64),
+        ("gmres_restart", ctypes.c_int32), ("ir_stall", ctypes.c_int32), ("gmres_tol", ctypes.c_double),
     ]
 
 
@@ -45,7 +47,8 @@ class LuResidualInfo(ctypes.Structure):
 class LuRefineInfo(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int32), ("gmres_iterations", ctypes.c_int32),
                 ("used_gmres", ctypes.c_int32), ("status", ctypes.c_int32),
-                ("r_hpl", ctypes.c_double), ("r_hpl_initial", ctypes.c_double), ("host_bytes", ctypes.c_int64)]
+                ("r_hpl", ctypes.c_double), ("r_hpl_initial", ctypes.c_double), ("host_bytes", ctypes.c_int64),
+                ("rejected", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 _lib = None
@@ -87,6 +90,7 @@ def load():
         "lu_refine_apply": ([H, P, i64, i32, P, i64, P, i64, i64, ctypes.POINTER(LuRefineInfo), P], ctypes.c_int),
         "lu_refine_adjoint": ([H, P, i64, P, i64, P, i64, i64, P, i64, P, i64, ctypes.POINTER(LuRefineInfo), P],
                               ctypes.c_int),
+        "lu_refine_precond_norm": ([H, P, i64, i32, ctypes.POINTER(ctypes.c_double), P], ctypes.c_int),
         "lu_batched_factor_solve": ([i32, P, P, P, P, P, P, i32, P, ctypes.c_size_t, P], ctypes.c_int),
         "lu_generate_uniform": ([P, i64, i64, i64, u64, u64, P], ctypes.c_int),
         "lu_matgen_host": ([P, i64, i32, i64], ctypes.c_int),
@@ -97,6 +101,7 @@ def load():
         "lu_solve_noalloc": ([P, i64, i64, P, P, P, P], ctypes.c_int),
         "lu_batched_work_bytes": ([i32, P, i32], ctypes.c_size_t),
         "lu_batched_set_tuning": ([i32, P], ctypes.c_int),
+        "lu_batched_refine_histogram": ([P, P, P], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

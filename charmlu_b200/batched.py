@@ -78,6 +78,20 @@ class BatchedSystems:
             raise RuntimeError(f"lu_batched_factor_solve failed ({rc})")
         return self.info
 
+    def refine_histogram(self, stream=None):
+        """After an FP32-mode factor_solve: systems that met r_hpl < 16
+        after s FP64 refinement steps, s = 0 .. 10, and (last entry) those
+        that did not (lu_batched_refine_histogram; synchronises)."""
+        L = _lib.load()
+        w = self.work(LU_PREC_FP32)
+        hist = np.zeros(12, dtype=np.int32)
+        s = stream if stream is not None else torch.cuda.current_stream()
+        rc = L.lu_batched_refine_histogram(ctypes.c_void_p(w.data_ptr()), ctypes.c_void_p(hist.ctypes.data),
+                                           ctypes.c_void_p(s.cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"lu_batched_refine_histogram failed ({rc})")
+        return hist
+
 
 def log_uniform_orders(count, lo=32, hi=1024, seed=42):
     """Orders drawn log-uniform in [lo, hi] from the seed."""

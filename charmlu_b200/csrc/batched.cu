@@ -63,12 +63,17 @@ struct BatchArgs {
 };
 
 // Workspace header written by the prep kernel (offsets in bytes from work).
+constexpr int kRefineHistBins = kBatchRefineMax + 2;  // steps 0 .. 10, then "not converged"
 struct WorkHeader {
   unsigned queue;
   int bad;          // nonzero: an order outside [1, kBatchMaxN] or workspace too small
   long long s1, s2; // sum n, sum n^2
   long long order, offA32, offV, piv, A32, r64, v32, total;
+  // FP32 mode: systems that reached r_hpl < 16 after s FP64 refinement
+  // steps (s = 0 .. 10), and in the last bin those that did not
+  int refine_hist[kRefineHistBins];
 };
+static_assert(sizeof(WorkHeader) <= 256, "workspace header exceeds its 256 bytes");
 
 __device__ __forceinline__ void tuning_for(int n, int esize, int& nb, int& small) {
   nb = esize == 8 ? 16 : 32;
@@ -519,11 +524,16 @@ __global__ void __launch_bounds__(BT, 1) batched_kernel(BatchArgs a) {
         const double r_hpl = rmax / ((anorm * xmax + bmax) * (double)n * 2.220446049250313e-16);
         if (isnan(r_hpl)) {
           if (info == 0) info = LU_ERR_NONFINITE;
+          if (tid == 0) atomicAdd(&hdr->refine_hist[kRefineHistBins - 1], 1);
           break;
         }
-        if (r_hpl < 16.0) break;
+        if (r_hpl < 16.0) {
+          if (tid == 0) atomicAdd(&hdr->refine_hist[step], 1);
+          break;
+        }
         if (step == kBatchRefineMax) {
           if (info == 0) info = LU_ERR_NOCONV;
+          if (tid == 0) atomicAdd(&hdr->refine_hist[kRefineHistBins - 1], 1);
           break;
         }
         if (tid == 0) {
@@ -590,6 +600,7 @@ __global__ void __launch_bounds__(1024) batched_prep_kernel(int count, const int
       if (v >= 1 && v <= kBatchMaxN) { s2 += (long long)v * v; s1 += v; }
     }
     hdr->queue = 0;
+    for (int q = 0; q < kRefineHistBins; q++) hdr->refine_hist[q] = 0;
     hdr->s1 = s1;
     hdr->s2 = s2;
     hdr->order = o_order;
@@ -647,6 +658,15 @@ extern "C" LU_API size_t lu_batched_work_bytes(int32_t count, const int32_t* n_h
     o = align256(o + 4 * s1);
   }
   return (size_t)o;
+}
+
+extern "C" LU_API int lu_batched_refine_histogram(const void* dWork, int32_t* hist, void* stream) {
+  if (!dWork || !hist) return LU_ERR_ARG;
+  const WorkHeader* hdr = static_cast<const WorkHeader*>(dWork);
+  cudaStream_t s = (cudaStream_t)stream;
+  LUB_CUDA(cudaMemcpyAsync(hist, hdr->refine_hist, sizeof(int) * kRefineHistBins, cudaMemcpyDeviceToHost, s));
+  LUB_CUDA(cudaStreamSynchronize(s));
+  return LU_OK;
 }
 
 extern "C" LU_API int lu_batched_set_tuning(int32_t entries, const int32_t* table) {

@@ -176,6 +176,11 @@ __global__ void multi_axpy_kernel(double* __restrict__ w, const double* __restri
   for (int j = 0; j < k; j++) t = fma(h[j], V[(int64_t)j * n + i], t);
   w[i] = fma(sign, t, w[i]);
 }
+// y = a * x
+__global__ void scale_vec_kernel(const double* __restrict__ x, double* __restrict__ y, int n, double a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = a * x[i];
+}
 // dst = src / sqrt(*sq)  (sq = squared norm)
 __global__ void scale_copy_kernel(const double* __restrict__ src, double* __restrict__ dst, int n,
                                   const double* __restrict__ sq) {
@@ -198,6 +203,12 @@ int launch_multi_dot(const double* V, int k, const double* w, int n, double* par
 int launch_multi_axpy(double* w, const double* V, int k, const double* h, int n, double sign, cudaStream_t s) {
   if (k <= 0) return LU_OK;
   multi_axpy_kernel<<<ceil_div(n, 256), 256, 0, s>>>(w, V, k, h, n, sign);
+  LUB_LAUNCH_CHECK();
+  return LU_OK;
+}
+int launch_scale_vec(const double* x, double* y, int n, double a, cudaStream_t s) {
+  if (n <= 0) return LU_OK;
+  scale_vec_kernel<<<ceil_div(n, 256), 256, 0, s>>>(x, y, n, a);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }

@@ -100,15 +100,94 @@ gemm_f32_sub_kernel(const float* __restrict__ A, int64_t lda, const float* __res
   }
 }
 
+// Narrow products (N <= BN <= 64, K <= 64: the deep halves of the recursive
+// panel and TRSM): the whole K x N operand B and a 64-row slice of A sit in
+// shared memory, and each thread keeps a (64 / row groups) x 4 block of C.
+// These launches are bound by the M x K and M x N traffic, which the 128 x
+// 128 tile above would spend mostly on zero-filled columns.  Each element is
+// accumulated over k in the same order and subtracted once, as above, so
+// both kernels give the same bits.
+constexpr int NBM = 64, NKMAX = 64, NTHREADS = 256;
+
+template <int BN>
+__global__ void __launch_bounds__(NTHREADS)
+gemm_f32_narrow_kernel(const float* __restrict__ A, int64_t lda, const float* __restrict__ B, int64_t ldb,
+                       float* __restrict__ C, int64_t ldc, int M, int N, int K) {
+  constexpr int QN = BN / 4;           // column quads
+  constexpr int RG = NTHREADS / QN;    // row groups
+  constexpr int RPT = NBM / RG;        // rows per thread
+  __shared__ __align__(16) float Bs[NKMAX][BN];
+  __shared__ float As[NBM][NKMAX + 1];
+  const int tid = threadIdx.x;
+  const int tx = tid % QN, ty = tid / QN;
+  const int row0 = blockIdx.x * NBM;
+  for (int idx = tid; idx < K * BN; idx += NTHREADS) {
+    const int k = idx / BN, c = idx - k * BN;
+    Bs[k][c] = c < N ? __ldg(&B[(int64_t)k * ldb + c]) : 0.f;
+  }
+  for (int idx = tid; idx < NBM * K; idx += NTHREADS) {
+    const int r = idx / K, k = idx - r * K;
+    As[r][k] = row0 + r < M ? __ldg(&A[(int64_t)(row0 + r) * lda + k]) : 0.f;
+  }
+  __syncthreads();
+  float acc[RPT][4];
+#pragma unroll
+  for (int i = 0; i < RPT; i++)
+#pragma unroll
+    for (int e = 0; e < 4; e++) acc[i][e] = 0.f;
+  for (int k = 0; k < K; k++) {
+    const float4 b = *reinterpret_cast<const float4*>(&Bs[k][tx * 4]);
+#pragma unroll
+    for (int i = 0; i < RPT; i++) {
+      const float a = As[ty + i * RG][k];
+      acc[i][0] = fmaf(a, b.x, acc[i][0]);
+      acc[i][1] = fmaf(a, b.y, acc[i][1]);
+      acc[i][2] = fmaf(a, b.z, acc[i][2]);
+      acc[i][3] = fmaf(a, b.w, acc[i][3]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < RPT; i++) {
+    const int r = row0 + ty + i * RG;
+    if (r >= M) continue;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const int c = tx * 4 + e;
+      if (c < N) C[(int64_t)r * ldc + c] -= acc[i][e];
+    }
+  }
+}
+
 }  // namespace
 
-int launch_gemm_f32_sub(const float* A, int64_t lda, const float* B, int64_t ldb, float* C, int64_t ldc, int M,
-                        int N, int K, cudaStream_t s) {
+static int gemm_f32_dispatch(const float* A, int64_t lda, const float* B, int64_t ldb, float* C, int64_t ldc, int M,
+                             int N, int K, bool allow_narrow, cudaStream_t s) {
   if (M <= 0 || N <= 0 || K <= 0) return LU_OK;
+  if (allow_narrow && K <= NKMAX && N <= 64) {
+    if (N <= 32)
+      gemm_f32_narrow_kernel<32><<<ceil_div(M, NBM), NTHREADS, 0, s>>>(A, lda, B, ldb, C, ldc, M, N, K);
+    else
+      gemm_f32_narrow_kernel<64><<<ceil_div(M, NBM), NTHREADS, 0, s>>>(A, lda, B, ldb, C, ldc, M, N, K);
+    LUB_LAUNCH_CHECK();
+    return LU_OK;
+  }
   dim3 grid(ceil_div(N, BN), ceil_div(M, BM));
   gemm_f32_sub_kernel<<<grid, THREADS, 0, s>>>(A, lda, B, ldb, C, ldc, M, N, K);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }
 
+int launch_gemm_f32_sub(const float* A, int64_t lda, const float* B, int64_t ldb, float* C, int64_t ldc, int M,
+                        int N, int K, cudaStream_t s) {
+  return gemm_f32_dispatch(A, lda, B, ldb, C, ldc, M, N, K, true, s);
+}
+
 }  // namespace lub
+
+// Test hook (not part of the ABI): C -= A B through the FP32 panel GEMM,
+// the narrow kernel where the shape allows it unless wide_only is set.
+extern "C" __attribute__((visibility("default"))) int lub_test_gemm_f32(const float* A, int64_t lda, const float* B,
+                                                                      int64_t ldb, float* C, int64_t ldc, int M,
+                                                                      int N, int K, int wide_only, void* stream) {
+  return lub::gemm_f32_dispatch(A, lda, B, ldb, C, ldc, M, N, K, wide_only == 0, (cudaStream_t)stream);
+}

@@ -4,6 +4,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "common.cuh"
@@ -95,9 +96,13 @@ struct lu_handle_s {
   double* r64 = nullptr;       // FP64 residual
   double* z64 = nullptr;       // FP64 work vector (GMRES)
   double* zero64 = nullptr;    // zeros (A v products through the residual kernel)
-  double* V = nullptr;         // GMRES basis, (gm+1) vectors of n
+  double* V = nullptr;         // GMRES Arnoldi basis, (gm+1) vectors of n (allocated on first use)
+  double* Z = nullptr;         // flexible GMRES: the preconditioned basis M^{-1} v_j, gm vectors of n
   double* hdot = nullptr;      // GMRES dot-product partials / results
   int gm = 0;                  // GMRES restart length
+  double* xbest = nullptr;     // refinement: the iterate with the smallest ||b - A x||inf so far
+  double* rbest = nullptr;     //   and its residual
+  lub::ResidualAccum* racc_best = nullptr;  //   and its norms
   bool mixed_ready = false;
   // factors kept for lu_refine_apply / lu_refine_adjoint
   bool mixed_factored = false;
@@ -111,6 +116,8 @@ struct lu_handle_s {
   double* mr_S = nullptr;      // GMRES: operand staging block (column 0 only)
   double* mr_T = nullptr;      // GMRES: product block
   double* mr_dc = nullptr;     // GMRES: correction of one column
+  double* mr_Xbest = nullptr;  // per column: the iterate with the smallest residual so far
+  double* mr_Rbest = nullptr;  //   and its residual
   unsigned long long* mr_acc = nullptr;
   // host-resident FP64 A (lu_refine_solve_host): row chunks staged through
   // two device buffers, copies on sCopy overlapping the kernels on the
@@ -145,6 +152,11 @@ struct lu_handle_s {
   cudaStream_t sG = nullptr;     // capture / replay stream
   cudaEvent_t evG0 = nullptr, evG1 = nullptr;
   bool capturing = false;
+  // kernel nodes the panel stream added during a capture: a captured kernel
+  // node does not keep its stream's priority, so run_graph gives them the
+  // panel stream's (highest) priority before instantiating the graph
+  std::vector<cudaGraphNode_t> prio_nodes;
+  int prio_hi = 0;
   // phase profiling (events on the launching stream)
   int profile = 0;
   struct Rec {
@@ -190,6 +202,40 @@ struct lu_handle_s {
 
 namespace lub {
 
+// The capture dependencies of stream s at this point of a capture.
+inline int capture_deps(cudaStream_t s, std::vector<cudaGraphNode_t>* out) {
+  cudaStreamCaptureStatus cs;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  LUB_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &nd));
+  out->assign(deps, deps + nd);
+  return LU_OK;
+}
+
+// During a capture: the kernel nodes stream s appended since its capture
+// dependencies were `before` (every node reachable backwards from its
+// current dependencies without passing a node of `before`) join
+// h->prio_nodes.
+inline int mark_branch_priority(lu_handle h, cudaStream_t s, const std::vector<cudaGraphNode_t>& before) {
+  std::vector<cudaGraphNode_t> todo, seen(before);
+  LUB_TRY(capture_deps(s, &todo));
+  while (!todo.empty()) {
+    cudaGraphNode_t nd = todo.back();
+    todo.pop_back();
+    if (std::find(seen.begin(), seen.end(), nd) != seen.end()) continue;
+    seen.push_back(nd);
+    cudaGraphNodeType t;
+    LUB_CUDA(cudaGraphNodeGetType(nd, &t));
+    if (t == cudaGraphNodeTypeKernel) h->prio_nodes.push_back(nd);
+    size_t np = 0;
+    LUB_CUDA(cudaGraphNodeGetDependencies(nd, nullptr, &np));
+    std::vector<cudaGraphNode_t> pred(np);
+    if (np) LUB_CUDA(cudaGraphNodeGetDependencies(nd, pred.data(), &np));
+    for (auto p : pred) todo.push_back(p);
+  }
+  return LU_OK;
+}
+
 // Brackets one phase with events when the handle is profiling.
 struct Prof {
   lu_handle h;
@@ -230,6 +276,7 @@ int run_graph(lu_handle h, int slot, const void* k1, const void* k2, const void*
     }
     LUB_CUDA(cudaStreamBeginCapture(h->sG, cudaStreamCaptureModeThreadLocal));
     h->capturing = true;
+    h->prio_nodes.clear();
     const long long before = __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED);
     const int rc = body(h->sG);
     // captured, not launched: the replays below count them
@@ -242,6 +289,17 @@ int run_graph(lu_handle h, int slot, const void* k1, const void* k2, const void*
       return rc;
     }
     LUB_CUDA(e);
+    for (auto nd : h->prio_nodes) {
+      cudaKernelNodeAttrValue v;
+      memset(&v, 0, sizeof(v));
+      v.priority = h->prio_hi;
+      if (cudaGraphKernelNodeSetAttribute(nd, cudaKernelNodeAttributePriority, &v) != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        h->prio_nodes.clear();
+        return LU_ERR_CUDA;
+      }
+    }
+    h->prio_nodes.clear();
     size_t nn = 0;
     cudaGraphGetNodes(graph, nullptr, &nn);
     std::vector<cudaGraphNode_t> nodes(nn);

@@ -100,6 +100,8 @@ int launch_multi_add(double* X, const double* D, const int32_t* perm, int n, int
 int launch_col_get(const double* M, int c, const int32_t* perm, double* out, int n, double scale, cudaStream_t s);
 int launch_vec_scatter(const double* src, const int32_t* perm, double* dst, int n, cudaStream_t s);
 int launch_col_put(double* M, int c, const double* v, int n, int assign, cudaStream_t s);
+// D[:, c] = S[:, c] (ld-16 blocks)
+int launch_col_copy(const double* S, double* D, int c, int n, cudaStream_t s);
 // G = -Lam X^T (rank k <= 16)
 int launch_neg_outer(const double* Lam, int64_t ldl, const double* X, int64_t ldx, int n, int k, double* G,
                      int64_t ldg, cudaStream_t s);
@@ -172,5 +174,7 @@ int launch_f32_to_f64(const float* y, double* x, int n, double scale, cudaStream
 int launch_multi_dot(const double* V, int k, const double* w, int n, double* part, double* out, cudaStream_t s);
 int launch_multi_axpy(double* w, const double* V, int k, const double* h, int n, double sign, cudaStream_t s);
 int launch_scale_copy(const double* src, double* dst, int n, const double* inv_of, cudaStream_t s);
+// y = a * x
+int launch_scale_vec(const double* x, double* y, int n, double a, cudaStream_t s);
 
 }  // namespace lub

@@ -202,9 +202,13 @@ int factor_f64_schedule(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, dou
   Ctx64 cp = c;
   cp.s = h->sP;
   cp.pl = h->plistP;
+  // under capture the panel stream's kernel nodes are marked for its priority
+  std::vector<cudaGraphNode_t> mark;
   LUB_CUDA(cudaEventRecord(h->evFork, s));
   LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evFork, 0));
+  if (h->capturing) LUB_TRY(capture_deps(h->sP, &mark));
   LUB_TRY(panel64(cp, 0, std::min(b, n), 0, std::min(b, n)));
+  if (h->capturing) LUB_TRY(mark_branch_priority(h, h->sP, mark));
   LUB_CUDA(cudaEventRecord(h->evP, h->sP));
   for (int k0 = 0; k0 < n; k0 += b) {
     const int kw = std::min(b, n - k0), k1 = k0 + kw, rest = n - k1;
@@ -216,7 +220,9 @@ int factor_f64_schedule(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, dou
     LUB_TRY(gemm64(c, c.A, k1, k1, c.A, k1, k0, c.A, k0, k1, rest, nw, kw, LU_PH_GEMM));  // next panel's columns
     LUB_CUDA(cudaEventRecord(h->evN, s));
     LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evN, 0));
+    if (h->capturing) LUB_TRY(capture_deps(h->sP, &mark));
     LUB_TRY(panel64(cp, k1, nw, k1, nw));
+    if (h->capturing) LUB_TRY(mark_branch_priority(h, h->sP, mark));
     LUB_CUDA(cudaEventRecord(h->evP, h->sP));
     if (rest > nw)
       LUB_TRY(gemm64(c, c.A, k1, k1 + nw, c.A, k1, k0, c.A, k0, k1 + nw, rest, rest - nw, kw, LU_PH_GEMM));
@@ -278,6 +284,9 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
   if (cfg->precision < LU_PREC_FP64 || cfg->precision > LU_PREC_FP16X3) return LU_ERR_ARG;
   if (cfg->layout != LU_LAYOUT_ROW && cfg->layout != LU_LAYOUT_COL) return LU_ERR_ARG;
   if (cfg->layout == LU_LAYOUT_COL && cfg->precision != LU_PREC_FP64) return LU_ERR_UNSUPPORTED;
+  if (cfg->gmres_restart < 0 || cfg->gmres_restart > 1000 || cfg->ir_stall < 0 || !(cfg->gmres_tol >= 0.0) ||
+      !(cfg->gmres_tol < 1.0))
+    return LU_ERR_ARG;
   LUB_TRY(ensure_kernels_init());
   lu_handle h = new lu_handle_s();
   h->cfg = *cfg;
@@ -308,6 +317,7 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
   if (s == LU_OK) {
     int lo = 0, hi = 0;
     cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    h->prio_hi = hi;
     if (cudaStreamCreateWithPriority(&h->sP, cudaStreamNonBlocking, hi) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->evP, cudaEventDisableTiming) != cudaSuccess ||
@@ -395,11 +405,15 @@ int lu_factor(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double* rhs, 
   if (h->cfg.precision != LU_PREC_FP64) return LU_ERR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
   if (h->cfg.layout != LU_LAYOUT_COL) return factor_f64(h, dA, lda, ipiv, rhs, s);
+  // every argument is checked before the first transpose, and a failure
+  // after it transposes back, so an error leaves the caller's matrix as given
   LUB_TRY(check_common(h, dA, lda));
+  if (!ipiv) return LU_ERR_ARG;
   const int n = (int)h->cfg.n;
   LUB_TRY(launch_transpose_inplace(dA, lda, n, s));
-  LUB_TRY(factor_f64(h, dA, lda, ipiv, rhs, s));
-  return launch_transpose_inplace(dA, lda, n, s);
+  const int rc = factor_f64(h, dA, lda, ipiv, rhs, s);
+  const int rc2 = launch_transpose_inplace(dA, lda, n, s);
+  return rc != LU_OK ? rc : rc2;
 }
 
 int lu_transpose_square(double* dA, int64_t n, int64_t lda, void* stream) {
@@ -469,13 +483,18 @@ int lu_factor_solve(lu_handle h, double* dA, int64_t lda, int32_t* ipiv, double*
   if (h->cfg.precision != LU_PREC_FP64) return LU_ERR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
   const bool col = h->cfg.layout == LU_LAYOUT_COL;
-  if (col) {
-    LUB_TRY(check_common(h, dA, lda));
-    LUB_TRY(launch_transpose_inplace(dA, lda, (int)h->cfg.n, s));
+  if (!col) {
+    LUB_TRY(factor_f64(h, dA, lda, ipiv, db, s));
+    return solve_permuted_f64(h, dA, lda, db, s);
   }
-  LUB_TRY(factor_f64(h, dA, lda, ipiv, db, s));
-  LUB_TRY(solve_permuted_f64(h, dA, lda, db, s));
-  return col ? launch_transpose_inplace(dA, lda, (int)h->cfg.n, s) : LU_OK;
+  // as lu_factor: check first, transpose back on every path after the first transpose
+  LUB_TRY(check_common(h, dA, lda));
+  if (!ipiv) return LU_ERR_ARG;
+  LUB_TRY(launch_transpose_inplace(dA, lda, (int)h->cfg.n, s));
+  int rc = factor_f64(h, dA, lda, ipiv, db, s);
+  if (rc == LU_OK) rc = solve_permuted_f64(h, dA, lda, db, s);
+  const int rc2 = launch_transpose_inplace(dA, lda, (int)h->cfg.n, s);
+  return rc != LU_OK ? rc : rc2;
 }
 
 int lu_residual(lu_handle h, const double* dA, int64_t lda, const double* dx, const double* db,

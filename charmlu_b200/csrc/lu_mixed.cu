@@ -9,9 +9,11 @@
 //                   subtracted into the FP32 matrix with TMA reduce-add
 //   refinement      FP64 residual r = b - A x against the untouched A, FP32
 //                   correction solve with the low-precision factors, FP64
-//                   update of x; classical IR first, GMRES-IR (left
-//                   preconditioned by the LU factors, FP64 Arnoldi) when the
-//                   classical iteration stops contracting.
+//                   update of x; classical IR first, GMRES-IR (flexible,
+//                   right preconditioned by the LU factors, FP64 Arnoldi)
+//                   when the classical iteration stops contracting.  A step
+//                   whose ||b - A x||inf is not below the best so far is
+//                   rolled back, so the reported residual never rises.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -22,7 +24,9 @@ using namespace lub;
 
 namespace {
 
-constexpr int kGmresRestart = 120;  // long Krylov spaces: short restarts stall when kappa * u_f >> 1
+constexpr int kGmresRestart = 120;  // default: long Krylov spaces, short restarts stall when kappa * u_f >> 1
+constexpr int kIrStall = 3;         // default: GMRES cycles in a row with < 10% progress before giving up
+constexpr double kGmresTol = 1e-10; // default: residual reduction that ends a GMRES cycle
 
 int ensure_mixed(lu_handle h) {
   if (h->mixed_ready) return LU_OK;
@@ -34,7 +38,7 @@ int ensure_mixed(lu_handle h) {
   h->pairs = h->cfg.precision == LU_PREC_FP16X3 && h->gemm_ctas > 0;
   h->nparts = h->cfg.precision == LU_PREC_FP16X3 ? (h->pairs ? 2 : 3) : 1;
   h->ldk = h->pairs ? 2 * ((B + 63) & ~int64_t(63)) : (h->nparts * B + 63) & ~int64_t(63);
-  h->gm = kGmresRestart;
+  h->gm = h->cfg.gmres_restart > 0 ? h->cfg.gmres_restart : kGmresRestart;
   LUB_TRY(h->alloc(&h->A32, (size_t)n * h->ld32));
   LUB_TRY(h->alloc(&h->Lb, (size_t)n * h->ldk));
   LUB_TRY(h->alloc(&h->Ub, (size_t)n * h->ldk));
@@ -50,11 +54,22 @@ int ensure_mixed(lu_handle h) {
   LUB_TRY(h->alloc(&h->r64, n));
   LUB_TRY(h->alloc(&h->z64, n));
   LUB_TRY(h->alloc(&h->zero64, n));
-  LUB_TRY(h->alloc(&h->V, (size_t)(h->gm + 1) * n));
-  LUB_TRY(h->alloc(&h->hdot, 128 * (h->gm + 2) + 2 * (h->gm + 2)));
+  LUB_TRY(h->alloc(&h->xbest, n));
+  LUB_TRY(h->alloc(&h->rbest, n));
+  LUB_TRY(h->alloc(&h->racc_best, 1));
   LUB_CUDA(cudaMemset(h->zero64, 0, sizeof(double) * n));
   h->mixed_ready = true;
   return LU_OK;
+}
+
+// The flexible GMRES work space: Arnoldi basis V, preconditioned basis Z
+// (about 2 * restart * n doubles; allocated on the first GMRES cycle)
+int ensure_gmres(lu_handle h) {
+  if (h->V) return LU_OK;
+  const size_t n = (size_t)h->cfg.n;
+  LUB_TRY(h->alloc(&h->V, (size_t)(h->gm + 1) * n));
+  LUB_TRY(h->alloc(&h->Z, (size_t)h->gm * n));
+  return h->alloc(&h->hdot, 128 * (h->gm + 2) + 2 * (h->gm + 2));
 }
 
 struct Ctx32 {
@@ -262,7 +277,10 @@ int factor_mixed_split_step(lu_handle h, Ctx32& c, Ctx32& cp, const CUtensorMap&
   LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, 0, nw, K, kpart, kw, false, s));  // next panel's columns
   LUB_CUDA(cudaEventRecord(h->evN, s));
   LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evN, 0));
+  std::vector<cudaGraphNode_t> mark;
+  if (h->capturing) LUB_TRY(capture_deps(h->sP, &mark));
   LUB_TRY(panel32(cp, k1, nw, k1, nw));
+  if (h->capturing) LUB_TRY(mark_branch_priority(h, h->sP, mark));
   // every other column: the left L columns, and the trailing ones past the
   // next panel (the panel's own columns are being factored beside this)
   LUB_TRY(pivots_apply_f32(c, k0, kw, 0, n, k0, k1 + nw, h->perm));
@@ -318,9 +336,13 @@ int factor_mixed(lu_handle h, cudaStream_t s) {
   Ctx32 cp = c;
   cp.s = h->sP;
   cp.pl = h->plistP;
+  // under capture the panel stream's kernel nodes are marked for its priority
+  std::vector<cudaGraphNode_t> mark;
   LUB_CUDA(cudaEventRecord(h->evFork, s));
   LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evFork, 0));
+  if (h->capturing) LUB_TRY(capture_deps(h->sP, &mark));
   LUB_TRY(panel32(cp, 0, std::min(B, n), 0, std::min(B, n)));
+  if (h->capturing) LUB_TRY(mark_branch_priority(h, h->sP, mark));
   LUB_CUDA(cudaEventRecord(h->evP, h->sP));
   const bool split = h->la_split && h->pairs && !bf16;
   for (int k0 = 0; k0 < n; k0 += B) {
@@ -340,7 +362,9 @@ int factor_mixed(lu_handle h, cudaStream_t s) {
     LUB_TRY(lowp_gemm(h, mapL, mapU, mapC, k1, rest, 0, nw, K, kpart, kw, bf16, s));  // next panel's columns
     LUB_CUDA(cudaEventRecord(h->evN, s));
     LUB_CUDA(cudaStreamWaitEvent(h->sP, h->evN, 0));
+    if (h->capturing) LUB_TRY(capture_deps(h->sP, &mark));
     LUB_TRY(panel32(cp, k1, nw, k1, nw));
+    if (h->capturing) LUB_TRY(mark_branch_priority(h, h->sP, mark));
     // The rest of update k runs on the SMs the panel leaves free; once the
     // panel is done, a helper launch on its stream takes the remaining
     // tiles from the same counter, so the reserved SMs do not idle.
@@ -498,18 +522,25 @@ int device_status(lu_handle h, cudaStream_t s) {
   return st.code != 0 ? st.code : st.info;
 }
 
-// Left-preconditioned GMRES on the correction: M^{-1} op(A) d = M^{-1} r
-// with M the FP32 factors applied in FP64 arithmetic (which GMRES-IR's
-// convergence needs), FP64 Arnoldi with two passes of classical
-// Gram-Schmidt.  x += d.
-//   init(v0):       v0 = M^{-1} (r / rnorm)
-//   op_prec(v, w):  w = M^{-1} op(A) v
-// rnorm: ||r||inf of the residual (the Krylov right-hand side is
-// beta * rnorm with beta = ||v0||2).
-template <class Init, class OpPrec>
-int gmres_cycle(lu_handle h, double* x, double rnorm, cudaStream_t s, int* iters_out, Init init, OpPrec op_prec) {
+// Flexible GMRES on the correction equation op(A) d = r, right
+// preconditioned: Arnoldi on op(A) M^{-1} in FP64 with two passes of
+// classical Gram-Schmidt, where M^{-1} (the FP32 factors applied in FP64
+// arithmetic) maps each basis vector v_j to z_j = M^{-1} v_j, kept in Z.  The
+// correction is d = Z y, with y minimising ||r - op(A) Z y||_2 over the
+// Krylov space, so each cycle minimises the true residual of the correction
+// equation (Saad, SIAM J. Sci. Comput. 14(2), 1993), not the preconditioned
+// one.  The cycle ends after gm steps or once that residual has fallen by
+// tol.  x += d.
+//   init(v0):    v0 = r / rnorm  (rnorm = ||r||inf keeps the vectors O(1))
+//   prec(v, z):  z = M^{-1} v
+//   op(z, w):    w = op(A) z
+template <class Init, class Prec, class Op>
+int fgmres_cycle(lu_handle h, double* x, double rnorm, double tol, cudaStream_t s, int* iters_out, Init init,
+                 Prec prec, Op op) {
+  LUB_TRY(ensure_gmres(h));
   const int n = (int)h->cfg.n, m = h->gm;
   double* V = h->V;
+  double* Z = h->Z;
   double* part = h->hdot;
   double* hd = h->hdot + 128 * (m + 2);  // m + 2 doubles of results
   std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1, 0.0), hcol(m + 1);
@@ -525,8 +556,10 @@ int gmres_cycle(lu_handle h, double* x, double rnorm, cudaStream_t s, int* iters
   int k = 0;
   for (int j = 0; j < m; j++) {
     double* vj = V + (size_t)j * n;
+    double* zj = Z + (size_t)j * n;
     double* w = V + (size_t)(j + 1) * n;
-    LUB_TRY(op_prec(vj, w));
+    LUB_TRY(prec(vj, zj));
+    LUB_TRY(op(zj, w));
     // two passes of classical Gram-Schmidt
     std::fill(hcol.begin(), hcol.end(), 0.0);
     for (int pass = 0; pass < 2; pass++) {
@@ -541,6 +574,7 @@ int gmres_cycle(lu_handle h, double* x, double rnorm, cudaStream_t s, int* iters
     double hn2 = 0.0;
     LUB_CUDA(cudaMemcpyAsync(&hn2, hd, sizeof(double), cudaMemcpyDeviceToHost, s));
     LUB_CUDA(cudaStreamSynchronize(s));
+    if (!std::isfinite(hn2)) break;  // keep the steps taken so far
     hcol[j + 1] = std::sqrt(hn2);
     if (hcol[j + 1] > 0.0) LUB_TRY(launch_scale_copy(w, w, n, hd, s));
     // Givens rotations
@@ -558,39 +592,49 @@ int gmres_cycle(lu_handle h, double* x, double rnorm, cudaStream_t s, int* iters
     g[j] = cs[j] * g[j];
     for (int i = 0; i <= j; i++) H[(size_t)i * m + j] = hcol[i];
     k = j + 1;
-    if (std::fabs(g[j + 1]) <= 1e-10 * beta * rnorm) break;
+    if (std::fabs(g[j + 1]) <= tol * beta * rnorm || !(hcol[j] > 0.0)) break;
   }
-  // y = H(1:k,1:k)^{-1} g(1:k); d = V y ; x += d
+  // y = H(1:k,1:k)^{-1} g(1:k); d = Z y; x += d
   std::vector<double> y(k, 0.0);
   for (int i = k - 1; i >= 0; i--) {
     double t = g[i];
     for (int q = i + 1; q < k; q++) t -= H[(size_t)i * m + q] * y[q];
-    y[i] = t / H[(size_t)i * m + i];
+    const double d = H[(size_t)i * m + i];
+    y[i] = d != 0.0 ? t / d : 0.0;
   }
-  LUB_CUDA(cudaMemcpyAsync(hd, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
-  LUB_TRY(launch_multi_axpy(x, V, k, hd, n, 1.0, s));
+  if (k > 0) {
+    LUB_CUDA(cudaMemcpyAsync(hd, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
+    LUB_TRY(launch_multi_axpy(x, Z, k, hd, n, 1.0, s));
+  }
   LUB_CUDA(cudaStreamSynchronize(s));
   *iters_out = k;
   return LU_OK;
+}
+
+double gmres_tol(lu_handle h) { return h->cfg.gmres_tol > 0.0 ? h->cfg.gmres_tol : kGmresTol; }
+int ir_stall_limit(lu_handle h) { return h->cfg.ir_stall > 0 ? h->cfg.ir_stall : kIrStall; }
+
+// z = M^{-1} v for the single-RHS solve: P, then the FP32 factors (FP64
+// vector and arithmetic)
+int prec_vec(lu_handle h, const int32_t* perm, const double* v, double* z, cudaStream_t s) {
+  LUB_TRY(launch_gather_f64(v, perm, z, (int)h->cfg.n, 1.0, nullptr, s));
+  return solve_f32_factors_f64(h, z, s);
 }
 
 // GMRES cycle of the single-RHS solve A x = b (residual in h->r64, its
 // norms in h->racc)
 int gmres_correction(lu_handle h, const ASrc& A, double* x, double rnorm, cudaStream_t s, int* iters_out) {
   const int n = (int)h->cfg.n;
-  auto init = [&](double* v0) {
-    LUB_TRY(launch_gather_f64(h->r64, h->perm, v0, n, 1.0, h->racc, s));
-    return solve_f32_factors_f64(h, v0, s);
-  };
-  auto op_prec = [&](const double* vj, double* w) {
-    {  // residual kernel with b = 0 gives -A v_j
+  auto init = [&](double* v0) { return launch_scale_vec(h->r64, v0, n, 1.0 / rnorm, s); };
+  auto prec = [&](const double* v, double* z) { return prec_vec(h, h->perm, v, z, s); };
+  auto op = [&](const double* z, double* w) {
+    {  // residual kernel with b = 0 gives -A z
       Prof pf(h, s, LU_PH_OTHER);
-      LUB_TRY(residual_src(h, A, vj, h->zero64, h->z64, s));
+      LUB_TRY(residual_src(h, A, z, h->zero64, h->z64, s));
     }
-    LUB_TRY(launch_gather_f64(h->z64, h->perm, w, n, -1.0, nullptr, s));
-    return solve_f32_factors_f64(h, w, s);
+    return launch_scale_vec(h->z64, w, n, -1.0, s);
   };
-  return gmres_cycle(h, x, rnorm, s, iters_out, init, op_prec);
+  return fgmres_cycle(h, x, rnorm, gmres_tol(h), s, iters_out, init, prec, op);
 }
 
 // FP32 working copy of A and its low-precision factorisation (h->A32,
@@ -650,21 +694,27 @@ int refine_solve(lu_handle h, const ASrc& A, const double* b, double* x, lu_refi
   }
   const double target = h->cfg.ir_target > 0 ? h->cfg.ir_target : 16.0;
   const int max_it = h->cfg.ir_max_iter > 0 ? h->cfg.ir_max_iter : 50;
+  const int stall_limit = ir_stall_limit(h);
   bool gm = h->cfg.ir_mode == LU_IR_GMRES;
-  double prev = INFINITY, r_hpl = INFINITY, rn = 0.0;
-  int it = 0, gm_stall = 0;
-  for (; it < max_it; it++) {
-    LUB_TRY(residual_hpl(h, A, x, b, h->r64, &r_hpl, &rn, s));
-    if (it == 0) ri.r_hpl_initial = r_hpl;
-    if (!std::isfinite(r_hpl)) break;
-    if (r_hpl < target) break;
-    if (!gm && it >= 2 && r_hpl > 0.5 * prev) gm = true;  // classical IR stopped contracting
-    // GMRES cycles that no longer reduce the residual: the low-precision
-    // factors have lost too much of A's spectrum; report non-convergence
-    if (ri.used_gmres) gm_stall = (r_hpl > 0.9 * prev) ? gm_stall + 1 : 0;
-    if (gm_stall >= 3) break;
-    prev = r_hpl;
-    if (gm) {
+  const size_t nb = sizeof(double) * (size_t)n;
+  // the iterate with the smallest ||b - A x||inf so far, its residual and
+  // norms: a step that does not lower that norm is rolled back to it
+  double r_hpl = INFINITY, rn = 0.0;
+  LUB_TRY(residual_hpl(h, A, x, b, h->r64, &r_hpl, &rn, s));
+  ri.r_hpl_initial = r_hpl;
+  double best_rn = rn, best_hpl = r_hpl;
+  auto save_best = [&]() -> int {
+    LUB_CUDA(cudaMemcpyAsync(h->xbest, x, nb, cudaMemcpyDeviceToDevice, s));
+    LUB_CUDA(cudaMemcpyAsync(h->rbest, h->r64, nb, cudaMemcpyDeviceToDevice, s));
+    LUB_CUDA(cudaMemcpyAsync(h->racc_best, h->racc, sizeof(ResidualAccum), cudaMemcpyDeviceToDevice, s));
+    return LU_OK;
+  };
+  LUB_TRY(save_best());
+  int stall = 0, steps = 0;
+  while (std::isfinite(r_hpl) && !(r_hpl < target) && steps < max_it) {
+    steps++;
+    const bool gm_step = gm;
+    if (gm_step) {
       int k = 0;
       LUB_TRY(gmres_correction(h, A, x, rn, s, &k));
       ri.used_gmres = 1;
@@ -675,6 +725,30 @@ int refine_solve(lu_handle h, const ASrc& A, const double* b, double* x, lu_refi
       LUB_TRY(launch_ir_update(x, h->v32, n, h->racc, s));
       ri.iterations++;
     }
+    double new_hpl = INFINITY, new_rn = INFINITY;
+    LUB_TRY(residual_hpl(h, A, x, b, h->r64, &new_hpl, &new_rn, s));
+    if (std::isfinite(new_rn) && new_rn < best_rn) {  // accepted
+      // classical steps that contract by less than 2x hand over to GMRES;
+      // GMRES cycles that gain less than 10% count towards the stall limit
+      if (!gm_step && !(new_hpl < 0.5 * best_hpl) && ri.iterations >= 2) gm = true;
+      if (gm_step) stall = (new_hpl > 0.9 * best_hpl) ? stall + 1 : 0;
+      best_rn = new_rn;
+      best_hpl = new_hpl;
+      r_hpl = new_hpl;
+      rn = new_rn;
+      LUB_TRY(save_best());
+    } else {  // rolled back to the best iterate and its residual
+      LUB_CUDA(cudaMemcpyAsync(x, h->xbest, nb, cudaMemcpyDeviceToDevice, s));
+      LUB_CUDA(cudaMemcpyAsync(h->r64, h->rbest, nb, cudaMemcpyDeviceToDevice, s));
+      LUB_CUDA(cudaMemcpyAsync(h->racc, h->racc_best, sizeof(ResidualAccum), cudaMemcpyDeviceToDevice, s));
+      r_hpl = best_hpl;
+      rn = best_rn;
+      ri.rejected++;
+      // a GMRES cycle from the same iterate would repeat itself: stop there
+      if (gm_step) break;
+      gm = true;
+    }
+    if (stall >= stall_limit) break;
   }
   ri.r_hpl = r_hpl;
   ri.status = (std::isfinite(r_hpl) && r_hpl < target) ? LU_OK : LU_ERR_NOCONV;
@@ -700,6 +774,8 @@ int ensure_multi(lu_handle h) {
   LUB_TRY(h->alloc(&h->mr_S, n * 16));
   LUB_TRY(h->alloc(&h->mr_T, n * 16));
   LUB_TRY(h->alloc(&h->mr_dc, n));
+  LUB_TRY(h->alloc(&h->mr_Xbest, n * 16));
+  LUB_TRY(h->alloc(&h->mr_Rbest, n * 16));
   LUB_TRY(h->alloc(&h->mr_acc, kMultiAccWords));
   LUB_CUDA(cudaMemset(h->mr_S, 0, sizeof(double) * n * 16));
   return LU_OK;
@@ -718,39 +794,35 @@ int prec_trans_vec(lu_handle h, double* v, double* tmp, cudaStream_t s) {
   return launch_vec_scatter(tmp, h->perm32, v, n, s);
 }
 
-// One GMRES cycle on column c of a refinement group: residual in
+// One flexible GMRES cycle on column c of a refinement group: residual in
 // h->mr_R[:, c] (||r||inf = rnorm), correction added to h->mr_X[:, c]
 int multi_gmres_column(lu_handle h, const double* A, int64_t lda, int trans, int c, double rnorm, int S,
                        int split_len, cudaStream_t s, int* iters) {
   const int n = (int)h->cfg.n;
-  auto init = [&](double* v0) {
-    if (!trans) {
-      LUB_TRY(launch_col_get(h->mr_R, c, h->perm32, v0, n, 1.0 / rnorm, s));
-      return solve_f32_factors_f64(h, v0, s);
-    }
-    LUB_TRY(launch_col_get(h->mr_R, c, nullptr, v0, n, 1.0 / rnorm, s));
-    return prec_trans_vec(h, v0, h->z64, s);
+  auto init = [&](double* v0) { return launch_col_get(h->mr_R, c, nullptr, v0, n, 1.0 / rnorm, s); };
+  auto prec = [&](const double* v, double* z) {
+    if (!trans) return prec_vec(h, h->perm32, v, z, s);
+    LUB_CUDA(cudaMemcpyAsync(z, v, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    return prec_trans_vec(h, z, h->z64, s);
   };
-  auto op_prec = [&](const double* vj, double* w) {
+  auto op = [&](const double* z, double* w) {
     if (!trans) {
-      {  // residual kernel with b = 0 gives -A v_j
+      {  // residual kernel with b = 0 gives -A z
         Prof pf(h, s, LU_PH_OTHER);
-        LUB_TRY(launch_residual_f64(A, lda, n, vj, h->zero64, h->z64, h->racc, s));
+        LUB_TRY(launch_residual_f64(A, lda, n, z, h->zero64, h->z64, h->racc, s));
       }
-      LUB_TRY(launch_gather_f64(h->z64, h->perm32, w, n, -1.0, nullptr, s));
-      return solve_f32_factors_f64(h, w, s);
+      return launch_scale_vec(h->z64, w, n, -1.0, s);
     }
-    LUB_TRY(launch_col_put(h->mr_S, 0, vj, n, 1, s));
-    {  // R = 0 - A^T v_j in column 0
+    LUB_TRY(launch_col_put(h->mr_S, 0, z, n, 1, s));
+    {  // R = 0 - A^T z in column 0
       Prof pf(h, s, LU_PH_OTHER);
       LUB_TRY(launch_multi_residual(A, lda, n, 1, h->mr_S, h->zero64, 1, 1, h->mr_T, h->mr_P, h->mr_Pn, S,
                                     split_len, 0, h->mr_acc, s));
     }
-    LUB_TRY(launch_col_get(h->mr_T, 0, nullptr, w, n, -1.0, s));
-    return prec_trans_vec(h, w, h->z64, s);
+    return launch_col_get(h->mr_T, 0, nullptr, w, n, -1.0, s);
   };
   LUB_CUDA(cudaMemsetAsync(h->mr_dc, 0, sizeof(double) * n, s));
-  LUB_TRY(gmres_cycle(h, h->mr_dc, rnorm, s, iters, init, op_prec));
+  LUB_TRY(fgmres_cycle(h, h->mr_dc, rnorm, gmres_tol(h), s, iters, init, prec, op));
   return launch_col_put(h->mr_X, c, h->mr_dc, n, 0, s);
 }
 
@@ -779,8 +851,11 @@ int multi_correction(lu_handle h, int trans, int k, cudaStream_t s) {
 // op(A) X = B for k <= 16 columns: low-precision solve, then classical IR
 // with the FP64 residual until every column's scaled residual is below the
 // target; when classical steps stop contracting (or cfg.ir_mode asks for
-// it) each column still above the target gets GMRES-IR cycles instead.
-// ri reports the worst column.
+// it) each column still above the target gets flexible GMRES-IR cycles
+// instead.  Per column, a step that does not lower ||r||inf is rolled back
+// to that column's best iterate (and a column whose GMRES cycle was rolled
+// back gets no further cycles: it would repeat itself).  ri reports the
+// worst column.
 int refine_group(lu_handle h, const double* A, int64_t lda, int trans, const double* B, int64_t ldb, double* X,
                  int64_t ldx, int k, lu_refine_info* ri, cudaStream_t s) {
   const int n = (int)h->cfg.n;
@@ -792,47 +867,86 @@ int refine_group(lu_handle h, const double* A, int64_t lda, int trans, const dou
   LUB_TRY(multi_correction(h, trans, k, s));
   const double target = h->cfg.ir_target > 0 ? h->cfg.ir_target : 16.0;
   const int max_it = h->cfg.ir_max_iter > 0 ? h->cfg.ir_max_iter : 50;
+  const int stall_limit = ir_stall_limit(h);
   const double eps = 2.220446049250313e-16;
-  double anorm = 0.0, prev = INFINITY, worst = INFINITY;
+  const size_t blk = sizeof(double) * (size_t)n * 16;
+  double anorm = 0.0;
   unsigned long long acc[kMultiAccWords];
-  double rc[16], rn[16];
+  double rc[16], rn[16], best_rn[16], best_rc[16];
+  bool frozen[16] = {};
   bool gm = h->cfg.ir_mode == LU_IR_GMRES;
-  int gm_stall = 0;
-  for (int it = 0;; it++) {
+  int stall = 0;
+  // residual of the current block and each column's scaled residual
+  auto residual = [&](bool first) -> int {
     {
       Prof pf(h, s, LU_PH_OTHER, 2.0 * n * (double)n * k);
       LUB_TRY(launch_multi_residual(A, lda, n, trans, h->mr_X, B, ldb, k, h->mr_R, h->mr_P, h->mr_Pn, S, split_len,
-                                    it == 0, h->mr_acc, s));
+                                    first ? 1 : 0, h->mr_acc, s));
     }
     LUB_CUDA(cudaMemcpyAsync(acc, h->mr_acc, sizeof(acc), cudaMemcpyDeviceToHost, s));
     LUB_CUDA(cudaStreamSynchronize(s));
-    if (it == 0) anorm = bits_to_double(acc[48]);
-    worst = 0.0;
+    if (first) anorm = bits_to_double(acc[48]);
     for (int c = 0; c < k; c++) {
       rn[c] = bits_to_double(acc[c]);
       rc[c] = rn[c] / ((anorm * bits_to_double(acc[32 + c]) + bits_to_double(acc[16 + c])) * (double)n * eps);
-      worst = (rc[c] > worst || std::isnan(rc[c])) ? rc[c] : worst;
     }
-    if (it == 0) ri->r_hpl_initial = std::max(ri->r_hpl_initial, worst);
-    if (!std::isfinite(worst) || worst < target || it >= max_it) break;
-    if (!gm && it >= 2 && worst > 0.5 * prev) gm = true;  // classical IR stopped contracting
-    // GMRES cycles that no longer reduce the residual: the low-precision
-    // factors have lost too much of A's spectrum; report non-convergence
-    if (ri->used_gmres) gm_stall = (worst > 0.9 * prev) ? gm_stall + 1 : 0;
-    if (gm_stall >= 3) break;
-    prev = worst;
-    if (gm) {
+    return LU_OK;
+  };
+  auto worst_of = [&](const double* v) {
+    double w = 0.0;
+    for (int c = 0; c < k; c++) w = (v[c] > w || std::isnan(v[c])) ? v[c] : w;
+    return w;
+  };
+  LUB_TRY(residual(true));
+  LUB_CUDA(cudaMemcpyAsync(h->mr_Xbest, h->mr_X, blk, cudaMemcpyDeviceToDevice, s));
+  LUB_CUDA(cudaMemcpyAsync(h->mr_Rbest, h->mr_R, blk, cudaMemcpyDeviceToDevice, s));
+  for (int c = 0; c < k; c++) {
+    best_rn[c] = std::isfinite(rn[c]) ? rn[c] : INFINITY;
+    best_rc[c] = rc[c];
+  }
+  double worst = worst_of(best_rc);
+  ri->r_hpl_initial = std::max(ri->r_hpl_initial, worst);
+  int classical = 0;
+  for (int it = 0; std::isfinite(worst) && !(worst < target) && it < max_it; it++) {
+    const bool gm_step = gm;
+    if (gm_step) {
+      bool any = false;
       for (int c = 0; c < k; c++) {
-        if (!(rc[c] >= target) || !(rn[c] > 0.0)) continue;
+        if (frozen[c] || !(best_rc[c] >= target) || !(best_rn[c] > 0.0)) continue;
         int iters = 0;
-        LUB_TRY(multi_gmres_column(h, A, lda, trans, c, rn[c], S, split_len, s, &iters));
+        LUB_TRY(multi_gmres_column(h, A, lda, trans, c, best_rn[c], S, split_len, s, &iters));
         ri->used_gmres = 1;
         ri->gmres_iterations += iters;
+        any = true;
       }
+      if (!any) break;
     } else {
       LUB_TRY(multi_correction(h, trans, k, s));
       ri->iterations++;
+      classical++;
     }
+    LUB_TRY(residual(false));
+    const double prev_worst = worst;
+    bool any_rejected = false;
+    for (int c = 0; c < k; c++) {
+      if (std::isfinite(rn[c]) && rn[c] < best_rn[c]) {  // accepted
+        best_rn[c] = rn[c];
+        best_rc[c] = rc[c];
+        LUB_TRY(launch_col_copy(h->mr_X, h->mr_Xbest, c, n, s));
+        LUB_TRY(launch_col_copy(h->mr_R, h->mr_Rbest, c, n, s));
+      } else if (best_rc[c] >= target) {  // rolled back (converged columns keep their best silently)
+        any_rejected = true;
+        ri->rejected++;
+        if (gm_step) frozen[c] = true;
+      }
+    }
+    // every column continues from its best iterate and residual
+    LUB_CUDA(cudaMemcpyAsync(h->mr_X, h->mr_Xbest, blk, cudaMemcpyDeviceToDevice, s));
+    LUB_CUDA(cudaMemcpyAsync(h->mr_R, h->mr_Rbest, blk, cudaMemcpyDeviceToDevice, s));
+    worst = worst_of(best_rc);
+    if (!gm_step && (any_rejected || (classical >= 2 && worst > 0.5 * prev_worst))) gm = true;
+    if (gm_step) stall = (worst > 0.9 * prev_worst) ? stall + 1 : 0;
+    if (stall >= stall_limit) break;
   }
   if (!(worst <= ri->r_hpl)) ri->r_hpl = worst;  // worst over groups (NaN sticks)
   if (!(std::isfinite(worst) && worst < target)) ri->status = LU_ERR_NOCONV;
@@ -916,6 +1030,49 @@ extern "C" int lu_refine_adjoint(lu_handle h, const double* dA, int64_t lda, con
     LUB_TRY(launch_neg_outer(gradB, ldgb, dX, ldx, n, (int)nrhs, gradA, ldga, s));
   }
   return LU_OK;
+}
+
+// Power iteration on E = I - M^{-1} A, M the low-precision factors of the
+// last lu_refine_factor (applied in FP64 arithmetic): v_{i+1} = E v_i /
+// ||E v_i||_2 from a seeded uniform start; *est receives ||E v||_2 for the
+// last unit v, a lower bound on ||E||_2 that approaches E's spectral radius.
+// Classical refinement contracts by about that factor per step (it
+// converges when it is below 1); GMRES-IR needs only M^{-1} A well enough
+// conditioned.
+extern "C" int lu_refine_precond_norm(lu_handle h, const double* dA, int64_t lda, int32_t iters, double* est,
+                                      void* stream) {
+  LUB_TRY(check_refine_args(h, dA, lda));
+  if (!est || iters < 1) return LU_ERR_ARG;
+  if ((lda & 1) || (reinterpret_cast<uintptr_t>(dA) & 15)) return LU_ERR_ALIGN;
+  if (!h->mixed_factored) return LU_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int n = (int)h->cfg.n;
+  LUB_TRY(ensure_gmres(h));
+  double* v = h->V;
+  double* w = h->V + n;
+  double* part = h->hdot;
+  double* hd = h->hdot + 128 * (h->gm + 2);
+  const double one = 1.0;
+  LUB_TRY(launch_gen_uniform(v, n, 1, 1, 20240601ULL, 7, s));
+  LUB_TRY(launch_multi_dot(v, 1, v, n, part, hd, s));
+  LUB_TRY(launch_scale_copy(v, v, n, hd, s));
+  double nrm = 0.0;
+  for (int i = 0; i < iters; i++) {
+    LUB_TRY(launch_residual_f64(dA, lda, n, v, h->zero64, h->z64, h->racc, s));  // z = -A v
+    LUB_TRY(prec_vec(h, h->perm32, h->z64, w, s));                              // w = -M^{-1} A v
+    LUB_CUDA(cudaMemcpyAsync(hd + 1, &one, sizeof(double), cudaMemcpyHostToDevice, s));
+    LUB_TRY(launch_multi_axpy(w, v, 1, hd + 1, n, 1.0, s));                      // w = v - M^{-1} A v
+    LUB_TRY(launch_multi_dot(w, 1, w, n, part, hd, s));
+    double sq = 0.0;
+    LUB_CUDA(cudaMemcpyAsync(&sq, hd, sizeof(double), cudaMemcpyDeviceToHost, s));
+    LUB_CUDA(cudaStreamSynchronize(s));
+    nrm = std::sqrt(sq);
+    if (!(nrm > 0.0) || !std::isfinite(nrm)) break;
+    LUB_TRY(launch_scale_copy(w, v, n, hd, s));
+  }
+  *est = nrm;
+  const int st = device_status(h, s);
+  return st < 0 ? st : LU_OK;
 }
 
 extern "C" int lu_refine_solve(lu_handle h, const double* dA, int64_t lda, const double* db, double* dx,

@@ -14,23 +14,24 @@
 //   the row swap on the rest of the panel's columns (the reference swaps
 //   whole rows of the panel block, lu.ci:302-323)
 //
-// Design: a cooperative grid of G CTAs, each holding a contiguous range of
-// the panel's rows in shared memory for the whole launch (row pitch W+1 so a
-// warp walking one column touches distinct banks).  Per column: each CTA
-// publishes its candidate (|value|, row, the row's W values) and, if it owns
-// row j, that row; one bounded grid barrier; every CTA reduces the G
-// candidates (warp shuffles), takes the pivot row from the winner's slot,
-// swaps locally, scales and updates its rows, and computes its candidate for
-// the next column in the same pass.  Slots are double-buffered by column
-// parity, which is safe because a CTA cannot reach barrier j+2 before every
-// CTA has left barrier j+1.
+// Design: a cooperative grid of G CTAs of NT threads, each holding a
+// contiguous range of the panel's rows in shared memory for the whole launch
+// (row pitch W+1 so a warp walking one column touches distinct banks).  Per
+// column: each CTA publishes its candidate (|value|, row, the row's W values)
+// and, if it owns row j, that row; one bounded grid barrier; then one round
+// trip to L2: while one warp reads the G candidate values and reduces them
+// (warp shuffles), the other threads read every candidate row and row j
+// into registers, so the pivot row is at hand as soon as the winner is
+// known.  Every CTA then swaps locally, scales and updates its rows, and
+// computes its candidate for the next column in the same pass.  Slots are
+// double-buffered by column parity, which is safe because a CTA cannot reach
+// barrier j+2 before every CTA has left barrier j+1.
 #include "common.cuh"
 #include "kernels.h"
 
 namespace lub {
 namespace {
 
-constexpr int THREADS = 256;
 // Columns are eliminated in groups of KG: a rank-1 update touches only the
 // rest of the current group, the columns past the group get one delayed
 // rank-KG update when the group ends, and a row that becomes a pivot row is
@@ -57,35 +58,46 @@ __device__ __forceinline__ void warp_argmax(T& v, int& r, int& w) {
   }
 }
 
-template <typename T>
+// s_v, s_r: NT/32 + 1 entries
+template <typename T, int NT>
 __device__ __forceinline__ void block_argmax(T v, int r, T* s_v, int* s_r, T& out_v, int& out_r) {
+  constexpr int NW = NT / 32;
   int w = 0;
   warp_argmax(v, r, w);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (lane == 0) { s_v[warp] = v; s_r[warp] = r; }
   __syncthreads();
   if (warp == 0) {
-    v = lane < THREADS / 32 ? s_v[lane] : T(0);
-    r = lane < THREADS / 32 ? s_r[lane] : -1;
+    v = lane < NW ? s_v[lane] : T(0);
+    r = lane < NW ? s_r[lane] : -1;
     warp_argmax(v, r, w);
-    if (lane == 0) { s_v[8] = v; s_r[8] = r; }
+    if (lane == 0) { s_v[NW] = v; s_r[NW] = r; }
   }
   __syncthreads();
-  out_v = s_v[8];
-  out_r = s_r[8];
+  out_v = s_v[NW];
+  out_r = s_r[NW];
 }
 
-template <typename T, int W>
-__global__ void __launch_bounds__(THREADS, 1)
+// Candidate rows read speculatively per thread after the barrier (G * W
+// values spread over the CTA); above this many per thread the pivot row is
+// read after the argmax instead (a second round trip).
+constexpr int kSpecPerThread = 2;
+
+template <typename T, int W, int NT>
+__global__ void __launch_bounds__(NT, 1)
 getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int row_base, LeafScratch<T> scr,
                   unsigned* bar, DevStatus* st, int info_base, double thr, long long spin, T* prow0, int pw,
                   int lc0) {
+  // rows a thread updates at once with explicit register staging (loads,
+  // then arithmetic, then stores), so their shared-memory round trips and
+  // divisions overlap: fewer when more threads share the rows
+  constexpr int RU = NT >= 1024 ? 1 : (NT >= 512 ? 2 : 4);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int LD = W + 1;
   T* a = reinterpret_cast<T*>(smem_raw);  // [R][LD]
   T* urow = a + (size_t)R * LD;           // [W] pivot row
-  __shared__ T s_v[9];
-  __shared__ int s_r[9];
+  __shared__ T s_v[NT / 32 + 1];
+  __shared__ int s_r[NT / 32 + 1];
   __shared__ int s_p, s_win;
   __shared__ T uhist[KG][W];     // pivot rows of the current group
   __shared__ unsigned s_scaled;  // group columns whose pivot was usable
@@ -95,7 +107,7 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
   const int r_hi = min(M, r_lo + R);
   const int nr = r_hi - r_lo;
 
-  for (int idx = tid; idx < nr * ncols; idx += THREADS) {
+  for (int idx = tid; idx < nr * ncols; idx += NT) {
     const int r = idx / ncols, c = idx - r * ncols;
     a[r * LD + c] = P[(int64_t)(r_lo + r) * lda + c];
   }
@@ -107,11 +119,11 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
   {
     T bv = 0;
     int br = -1;
-    for (int r = tid; r < nr; r += THREADS) {
+    for (int r = tid; r < nr; r += NT) {
       T v = fabs(a[r * LD]);
       if (v > bv) { bv = v; br = r_lo + r; }
     }
-    block_argmax(bv, br, s_v, s_r, cv, cr);
+    block_argmax<T, NT>(bv, br, s_v, s_r, cv, cr);
   }
 
   for (int j = 0; j < ncols; j++) {
@@ -129,7 +141,25 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
     // these writes visible to every CTA that passes the barrier
     if (!grid_barrier(bar, (unsigned)(j + 1) * (unsigned)G, st, spin, 201)) return;
 
-    // ---- global argmax over the G candidates
+    // ---- global argmax over the G candidates; meanwhile the other threads
+    //      read every candidate row (and row j) from the same round trip
+    const bool spec = G * ncols <= kSpecPerThread * NT;
+    T sv[kSpecPerThread];
+    int sq[kSpecPerThread];
+    T rj = T(0);
+    if (spec) {
+#pragma unroll
+      for (int e = 0; e < kSpecPerThread; e++) {
+        const int idx = tid + e * NT;
+        sq[e] = -1;
+        if (idx < G * ncols) {
+          const int q = idx / ncols, c = idx - q * ncols;
+          sq[e] = q;
+          sv[e] = __ldcg(&scr.cand_data[((size_t)slot * kMaxLeafCTAs + q) * kMaxLeafW + c]);
+        }
+      }
+    }
+    if (tid < ncols) rj = __ldcg(&scr.rowj[slot * kMaxLeafW + tid]);
     if (tid < 32) {
       T v = 0;
       int r = -1, w = 0;
@@ -144,9 +174,14 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
     __syncthreads();
     const bool zero_col = s_p < 0;
     const int p = zero_col ? j : s_p;
-    if (tid < ncols) {
-      urow[tid] = zero_col ? __ldcg(&scr.rowj[slot * kMaxLeafW + tid])
-                           : __ldcg(&scr.cand_data[((size_t)slot * kMaxLeafCTAs + s_win) * kMaxLeafW + tid]);
+    if (zero_col) {
+      if (tid < ncols) urow[tid] = rj;
+    } else if (spec) {
+#pragma unroll
+      for (int e = 0; e < kSpecPerThread; e++)
+        if (sq[e] == s_win) urow[tid + e * NT - s_win * ncols] = sv[e];
+    } else if (tid < ncols) {
+      urow[tid] = __ldcg(&scr.cand_data[((size_t)slot * kMaxLeafCTAs + s_win) * kMaxLeafW + tid]);
     }
     __syncthreads();
     // the pivot row's columns past the group still lack the group's earlier
@@ -163,7 +198,7 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
       __syncthreads();
     }
     if (tid < ncols) {
-      if (p != j && p >= r_lo && p < r_hi) a[(p - r_lo) * LD + tid] = __ldcg(&scr.rowj[slot * kMaxLeafW + tid]);
+      if (p != j && p >= r_lo && p < r_hi) a[(p - r_lo) * LD + tid] = rj;
       // position j takes the (brought up to date) pivot row, also when p == j
       if (j >= r_lo && j < r_hi) a[(j - r_lo) * LD + tid] = urow[tid];
     }
@@ -176,7 +211,7 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
       const int q0 = cta * per, q1 = min(others, q0 + per);
       T* r1 = prow0 + (int64_t)j * lda;
       T* r2 = prow0 + (int64_t)p * lda;
-      for (int q = q0 + tid; q < q1; q += THREADS) {
+      for (int q = q0 + tid; q < q1; q += NT) {
         const int col = q < lc0 ? q : q + ncols;
         const T t = r1[col];
         r1[col] = r2[col];
@@ -201,16 +236,13 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
     T bv = 0;
     int br = -1;
     const int r_first = max(j + 1 - r_lo, 0);
-    // pivot-row values are warp-wide broadcasts.  A thread works on RU rows
-    // at once with explicit register staging (loads, then arithmetic, then
-    // stores), so the rows' shared-memory round trips and divisions overlap.
-    constexpr int RU = 4;
-    for (int rb = r_first + tid; rb < nr; rb += THREADS * RU) {
+    // pivot-row values are warp-wide broadcasts; RU rows per thread at once
+    for (int rb = r_first + tid; rb < nr; rb += NT * RU) {
       T* rp[RU];
       bool live[RU];
 #pragma unroll
       for (int u = 0; u < RU; u++) {
-        const int r = rb + u * THREADS;
+        const int r = rb + u * NT;
         live[u] = r < nr;
         rp[u] = a + (size_t)(live[u] ? r : rb) * LD;
       }
@@ -264,15 +296,15 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
         for (int u = 0; u < RU; u++) {
           if (live[u]) {
             const T v = fabs(rp[u][j + 1]);
-            if (v > bv) { bv = v; br = r_lo + rb + u * THREADS; }
+            if (v > bv) { bv = v; br = r_lo + rb + u * NT; }
           }
         }
       }
     }
-    block_argmax(bv, br, s_v, s_r, cv, cr);
+    block_argmax<T, NT>(bv, br, s_v, s_r, cv, cr);
   }
 
-  for (int idx = tid; idx < nr * ncols; idx += THREADS) {
+  for (int idx = tid; idx < nr * ncols; idx += NT) {
     const int r = idx / ncols, c = idx - r * ncols;
     P[(int64_t)(r_lo + r) * lda + c] = a[r * LD + c];
   }
@@ -280,6 +312,16 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
 
 template <typename T, int W>
 size_t leaf_smem(int R) { return (size_t)R * (W + 1) * sizeof(T) + W * sizeof(T); }
+
+// threads per leaf CTA: 256, 512 or 1024 (LU_B200_LEAF_THREADS, read once)
+int leaf_threads() {
+  static int nt = [] {
+    const char* e = getenv("LU_B200_LEAF_THREADS");
+    const int v = e ? atoi(e) : 1024;
+    return v >= 1024 ? 1024 : (v >= 512 ? 512 : 256);
+  }();
+  return nt;
+}
 
 template <typename T, int W>
 int launch_leaf_w(T* P, int64_t lda, int M, int ncols, int32_t* ipiv, int row_base, const LeafScratch<T>& scr,
@@ -299,19 +341,33 @@ int launch_leaf_w(T* P, int64_t lda, int M, int ncols, int32_t* ipiv, int row_ba
   size_t smem = leaf_smem<T, W>(R);
   void* args[] = {&P, &lda, &M, &ncols, &R, &ipiv, &row_base, const_cast<LeafScratch<T>*>(&scr), &bar, &st,
                   &info_base, &thr, &spin, &prow0, &pw, &lc0};
-  LUB_CUDA(cudaLaunchCooperativeKernel((const void*)getf2_leaf_kernel<T, W>, dim3(G), dim3(THREADS), args, smem, s));
+  const int nt = leaf_threads();
+  const void* fn = nt == 1024 ? (const void*)getf2_leaf_kernel<T, W, 1024>
+                              : (nt == 512 ? (const void*)getf2_leaf_kernel<T, W, 512>
+                                           : (const void*)getf2_leaf_kernel<T, W, 256>);
+  LUB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(nt), args, smem, s));
   __atomic_add_fetch(&g_kernel_launches, 1, __ATOMIC_RELAXED);
   return LU_OK;
 }
 
 }  // namespace
 
+template <typename T, int NT>
+int leaf_init_nt() {
+  LUB_CUDA(cudaFuncSetAttribute(getf2_leaf_kernel<T, 16, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                220 * 1024));
+  LUB_CUDA(cudaFuncSetAttribute(getf2_leaf_kernel<T, 32, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                220 * 1024));
+  LUB_CUDA(cudaFuncSetAttribute(getf2_leaf_kernel<T, 64, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                220 * 1024));
+  return LU_OK;
+}
+
 template <typename T>
 int leaf_init() {
-  LUB_CUDA(cudaFuncSetAttribute(getf2_leaf_kernel<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-  LUB_CUDA(cudaFuncSetAttribute(getf2_leaf_kernel<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-  LUB_CUDA(cudaFuncSetAttribute(getf2_leaf_kernel<T, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-  return LU_OK;
+  LUB_TRY((leaf_init_nt<T, 256>()));
+  LUB_TRY((leaf_init_nt<T, 512>()));
+  return leaf_init_nt<T, 1024>();
 }
 
 // ncols <= 64; the kernel instance is the narrowest of 16/32/64 that holds

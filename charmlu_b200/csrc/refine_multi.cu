@@ -210,6 +210,11 @@ __global__ void vec_scatter_kernel(const double* src, const int32_t* perm, doubl
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) dst[perm[i]] = src[i];
 }
+// D[i][c] = S[i][c] for one column of two ld-16 blocks
+__global__ void col_copy_kernel(const double* S, double* D, int c, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) D[(int64_t)i * 16 + c] = S[(int64_t)i * 16 + c];
+}
 // M[i][c] = v[i] (assign) or M[i][c] += v[i]; M ld 16
 __global__ void col_put_kernel(double* M, int c, const double* v, int n, int assign) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -282,6 +287,13 @@ int launch_col_get(const double* M, int c, const int32_t* perm, double* out, int
 int launch_vec_scatter(const double* src, const int32_t* perm, double* dst, int n, cudaStream_t s) {
   if (n <= 0) return LU_OK;
   vec_scatter_kernel<<<ceil_div(n, 256), 256, 0, s>>>(src, perm, dst, n);
+  LUB_LAUNCH_CHECK();
+  return LU_OK;
+}
+
+int launch_col_copy(const double* S, double* D, int c, int n, cudaStream_t s) {
+  if (n <= 0) return LU_OK;
+  col_copy_kernel<<<ceil_div(n, 256), 256, 0, s>>>(S, D, c, n);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }

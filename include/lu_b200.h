@@ -93,6 +93,10 @@ typedef struct lu_config {
   double  sing_threshold;  /* |u_jj| <= threshold sets info; the reference aborts at 100*eps (lu.ci:339) */
   double  ir_target;       /* refinement stops when r_hpl < ir_target (default 16) */
   int64_t spin_limit;      /* bounded-wait iteration cap for cross-CTA waits (0 = default) */
+  int32_t gmres_restart;   /* GMRES-IR: Krylov vectors per cycle (0 = 120) */
+  int32_t ir_stall;        /* refinement gives up (LU_ERR_NOCONV) after this many GMRES cycles in a row
+                              that cut the scaled residual by less than 10% (0 = 3) */
+  double  gmres_tol;       /* GMRES-IR: a cycle ends once ||r - op(A) d||_2 has fallen by this factor (0 = 1e-10) */
 } lu_config;
 
 typedef struct lu_handle_s* lu_handle;
@@ -117,6 +121,8 @@ typedef struct lu_refine_info {
   double  r_hpl;             /* final scaled residual */
   double  r_hpl_initial;     /* scaled residual of the low-precision solve */
   int64_t host_bytes;        /* bytes of A copied host -> device (lu_refine_solve_host; else 0) */
+  int32_t rejected;          /* refinement steps rolled back because ||b - A x||inf did not fall */
+  int32_t reserved;
 } lu_refine_info;
 
 /* Fill *cfg with defaults for order n and block size b (LUConfig defaults,
@@ -218,6 +224,16 @@ LU_API int lu_refine_apply(lu_handle h, const double* dA, int64_t lda, int trans
                     int64_t ldb, double* dX, int64_t ldx, int64_t nrhs, lu_refine_info* info,
                     void* stream);
 
+/* Estimate of ||I - M^{-1} A|| for the low-precision factors M of the last
+ * lu_refine_factor (no reference counterpart): iters steps of power
+ * iteration on I - M^{-1} A (M^{-1} applied in FP64 arithmetic on the FP32
+ * factors) from a seeded start; *est receives the last step's growth
+ * factor, a lower bound on the 2-norm that approaches the spectral radius.
+ * Classical refinement contracts by about *est per step and converges when
+ * it is below 1.  dA: the FP64 matrix the factors came from.  Synchronises. */
+LU_API int lu_refine_precond_norm(lu_handle h, const double* dA, int64_t lda, int32_t iters, double* est,
+                                  void* stream);
+
 /* Adjoint of X = A^{-1} B on low-precision factors (no reference
  * counterpart): lambda = A^{-T} W by lu_refine_apply (trans = 1) into
  * gradB, then grad_A = -lambda X^T into gradA (n x n, ldga; may be NULL).
@@ -252,6 +268,12 @@ LU_API int lu_batched_factor_solve(int32_t count, const int32_t* n, const int64_
                             int32_t precision, void* dWork, size_t work_bytes, void* stream);
 /* Scratch bytes lu_batched_factor_solve needs for these orders (n_host: host array). */
 LU_API size_t lu_batched_work_bytes(int32_t count, const int32_t* n_host, int32_t precision);
+/* After an LU_PREC_FP32 lu_batched_factor_solve on dWork (device), once the
+ * stream reaches it: hist[s] (host, 12 entries) = systems whose scaled
+ * residual was below 16 after s FP64 refinement steps (s = 0 .. 10; the
+ * north star's one step is s = 1), hist[11] = systems that did not get
+ * there.  Synchronises.  No reference counterpart. */
+LU_API int lu_batched_refine_histogram(const void* dWork, int32_t* hist, void* stream);
 /* Per-size-bucket kernel parameters chosen by the autotuner: entries of
  * {n_max, panel_width, small_threshold} (host array, ascending n_max, at most
  * 16); count 0 restores the built-in defaults.  Applies to later batched
@@ -357,16 +379,19 @@ LU_API int lu_copy_2d(void* dst, int64_t dpitch, const void* src, int64_t spitch
 LU_API int64_t lu_launch_count(void);
 
 /* Solve without allocating (no counterpart in the reference).  For callers
- * that cannot call cudaMalloc — code running inside a CUDA graph capture, a
- * host with a fixed device-memory budget, or a caller without a handle.
+ * that may not call cudaMalloc: a plugin whose host application owns the
+ * device memory and grants a fixed budget, a real-time loop that cannot
+ * afford an allocation's device-wide synchronisation, or a caller without a
+ * handle (lu_create allocates).
  * Same result as lu_solve(h, dLU, lda, ipiv, db, 1, 1, 0, stream): x =
  * A^{-1} b from lu_factor's factors and pivots, db (device) overwritten.
  * Scratch lives in a fixed ~8 KB device array inside the library (held by
  * every GPU that loads it until exit), so n is limited to 131072; larger n
  * returns LU_ERR_ARG.  d_status (optional, device int) receives LU_OK or
  * LU_ERR_TIMEOUT.  The first call on a device resolves the array's address
- * and should come before any stream capture.  Calls share the array: calls
- * that overlap on the GPU race. */
+ * and should come before any stream capture; the address is cached and does
+ * not survive a device reset.  Calls share the array: calls that overlap on
+ * the GPU race. */
 LU_API int lu_solve_noalloc(const double* dLU, int64_t lda, int64_t n, const int32_t* ipiv, double* db,
                             int32_t* d_status, void* stream);
 

@@ -98,3 +98,38 @@ def test_bindings_match_header_parameter_counts():
     for name, k in counts.items():
         argtypes = getattr(L, name).argtypes
         assert argtypes is not None and len(argtypes) == k, (name, k, argtypes)
+
+
+def test_create_rejects_bad_refinement_settings_without_gpu():
+    from charmlu_b200 import _lib
+    L = _lib.load()
+    h = ctypes.c_void_p()
+    for field, bad in (("gmres_restart", -1), ("gmres_restart", 5000), ("ir_stall", -2), ("gmres_tol", 1.5),
+                       ("gmres_tol", -1e-3), ("gmres_tol", float("nan"))):
+        c = _lib.LuConfig()
+        L.lu_config_default(ctypes.byref(c), 256, 64)
+        setattr(c, field, bad)
+        assert L.lu_create(ctypes.byref(c), ctypes.byref(h)) == -1, (field, bad)
+
+
+def test_config_struct_layout_matches_header():
+    """sizeof and field offsets of lu_config / lu_refine_info as the C
+    compiler lays them out equal the ctypes mirrors'."""
+    import tempfile
+    from charmlu_b200 import _lib
+    fields = {"lu_config": _lib.LuConfig, "lu_refine_info": _lib.LuRefineInfo}
+    src = ["#include <stdio.h>", "#include <stddef.h>", '#include "lu_b200.h"', "int main(void) {"]
+    for name, cls in fields.items():
+        src.append(f'printf("{name} %zu\\n", sizeof({name}));')
+        for f, _ in cls._fields_:
+            src.append(f'printf("{name}.{f} %zu\\n", offsetof({name}, {f}));')
+    src.append("return 0; }")
+    with tempfile.TemporaryDirectory() as d:
+        c_path, exe = os.path.join(d, "layout.c"), os.path.join(d, "layout")
+        open(c_path, "w").write("\n".join(src))
+        subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), c_path, "-o", exe])
+        out = dict(line.split() for line in subprocess.check_output([exe], text=True).splitlines())
+    for name, cls in fields.items():
+        assert int(out[name]) == ctypes.sizeof(cls), name
+        for f, _ in cls._fields_:
+            assert int(out[f"{name}.{f}"]) == getattr(cls, f).offset, (name, f)

@@ -45,6 +45,12 @@ def _run(n, a_off, b_off, precision, seed=42):
                                    ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
     torch.cuda.synchronize()
     assert rc == 0
+    if precision == LU_PREC_FP32:
+        # every system lands in exactly one bin of the refinement-step histogram
+        hist = np.zeros(12, dtype=np.int32)
+        assert L.lu_batched_refine_histogram(ctypes.c_void_p(work.data_ptr()), ctypes.c_void_p(hist.ctypes.data),
+                                             ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
+        assert hist.sum() == count and hist[11] == int((info.cpu().numpy() != 0).sum()), hist
     return A0.cpu().numpy(), b0.cpu().numpy(), b.cpu().numpy(), info.cpu().numpy(), A
 
 

@@ -343,3 +343,108 @@ def test_refine_solve_host_matches_device(cuda_dev, n, b, stage, resident, monke
     assert torch.equal(x2, x_dev) and i2["host_bytes"] == i_host["host_bytes"]
     with pytest.raises(lu.LUError):
         s.refine_solve_host(A, bvec)  # a device tensor is rejected
+
+
+@pytest.mark.parametrize("kappa", [1e6, 1e10])
+@pytest.mark.parametrize("prec", [1, 2, 3])
+def test_refinement_never_raises_the_residual(cuda_dev, kappa, prec):
+    """Hard systems for the low-precision factors: whatever the outcome, the
+    returned x has the smallest residual the refinement reached (steps that
+    raise ||b - A x||inf are rolled back), its r_hpl is what info reports,
+    and non-convergence is reported as LU_ERR_NOCONV."""
+    import sys, os
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from bench import kappa_matrix
+    import charmlu_b200 as lu
+    n = 1024
+    A = kappa_matrix(n, kappa, 5, torch.device("cuda"))
+    b = lu.generate_uniform(n, 1, seed=43, stream_id=1).view(-1)
+    s = lu.LUSolver(lu.LUConfig(n, 256, precision=prec, ir_max_iter=20, gmres_restart=60))
+    x, info = s.refine_solve(A, b)
+    st = s.status()
+    assert info["r_hpl"] <= info["r_hpl_initial"], info
+    r = s.residual(A, x, b)
+    assert abs(r["r_hpl"] - info["r_hpl"]) <= 1e-6 * max(1.0, info["r_hpl"]), (r, info)
+    if st == 0:
+        assert info["r_hpl"] < 16
+    else:
+        assert st == lu.LU_ERR_NOCONV and info["status"] == lu.LU_ERR_NOCONV
+
+
+def test_refine_apply_never_raises_the_residual(cuda_dev):
+    """The multi-RHS refinement (both op(A) = A and A^T) keeps each column's
+    best iterate."""
+    import sys, os
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from bench import kappa_matrix
+    import charmlu_b200 as lu
+    n = 1024
+    A = kappa_matrix(n, 1e6, 6, torch.device("cuda"))
+    B = lu.generate_uniform(n, 5, seed=44, stream_id=2)
+    s = lu.LUSolver(lu.LUConfig(n, 256, precision=lu.LU_PREC_BF16, ir_max_iter=15, gmres_restart=40))
+    s.refine_factor(A)
+    for trans in (False, True):
+        X, info = s.refine_apply(A, B, trans=trans)
+        assert info["r_hpl"] <= info["r_hpl_initial"], info
+        if info["status"] == 0:
+            op = A.t() if trans else A
+            R = B - op @ X
+            an = op.abs().sum(dim=1).max()
+            for c in range(5):
+                rc = R[:, c].abs().max() / ((an * X[:, c].abs().max() + B[:, c].abs().max()) * n * 2.22e-16)
+                assert rc.item() < 16
+
+
+def test_precond_norm_estimate(cuda_dev):
+    """||I - M^{-1} A||: well below 1 for the near-FP32 FP16x3 factors of a
+    well-conditioned matrix (classical refinement contracts fast), larger
+    for BF16 factors of an ill-conditioned one; cross-checked against the
+    contraction the refinement shows."""
+    import sys, os
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from bench import kappa_matrix
+    import charmlu_b200 as lu
+    n = 1024
+    A = kappa_matrix(n, 1e2, 7, torch.device("cuda"))
+    s = lu.LUSolver(lu.LUConfig(n, 256, precision=lu.LU_PREC_FP16X3))
+    s.refine_factor(A)
+    e3 = s.refine_precond_norm(A, iters=12)
+    assert 0.0 < e3 < 1e-2, e3
+    A6 = kappa_matrix(n, 1e6, 7, torch.device("cuda"))
+    s6 = lu.LUSolver(lu.LUConfig(n, 256, precision=lu.LU_PREC_BF16))
+    s6.refine_factor(A6)
+    e6 = s6.refine_precond_norm(A6, iters=12)
+    assert e6 > 10 * e3 and np.isfinite(e6), (e3, e6)
+    with pytest.raises(lu.LUError):
+        lu.LUSolver(lu.LUConfig(n, 256, precision=lu.LU_PREC_BF16)).refine_precond_norm(A, iters=4)
+
+
+@pytest.mark.parametrize("M,N,K", [(32768, 32, 32), (4096, 64, 64), (1000, 48, 16), (77, 2, 4), (5000, 128, 128),
+                                   (3000, 200, 96)])
+def test_gemm_f32_panel_kernels_match_torch(cuda_dev, M, N, K):
+    """The FP32 panel GEMM (C -= A B) against a plain FP32 torch product, and
+    the narrow kernel (N, K <= 64) against the 128 x 128 tile kernel: both
+    accumulate over k in order and subtract once, so they agree bit for
+    bit."""
+    from charmlu_b200 import _lib as L
+    f = L.load().lub_test_gemm_f32
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                  ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    f.restype = ctypes.c_int
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    A = torch.rand(M, K + 3, device="cuda", generator=g)[:, :K] - 0.5  # row pitch != K
+    B = torch.rand(K, N + 1, device="cuda", generator=g)[:, :N] - 0.5
+    C0 = torch.rand(M, N + 5, device="cuda", generator=g) - 0.5
+    out = []
+    for wide_only in (0, 1):
+        Cb = C0.clone()
+        C = Cb[:, :N]
+        st = torch.cuda.current_stream().cuda_stream
+        assert f(A.data_ptr(), A.stride(0), B.data_ptr(), B.stride(0), C.data_ptr(), C.stride(0), M, N, K,
+                 wide_only, st) == 0
+        torch.cuda.synchronize()
+        assert torch.equal(Cb[:, N:], C0[:, N:])  # nothing right of C touched
+        out.append(C.clone())
+    ref = C0[:, :N].double() - A.double() @ B.double()
+    assert (out[0].double() - ref).abs().max().item() <= 4e-7 * K
+    assert torch.equal(out[0], out[1])
