@@ -392,10 +392,22 @@ def run_ksweep(args, rank, world):
             st = s.status()
             r = s.residual(A, x, b)
             fe = float(np.abs(x.cpu().numpy() - x_ref).max() / np.abs(x_ref).max())
+            # ||I - M^{-1} A|| of these factors (power iteration on the kept
+            # factors of a separate refine_factor): classical refinement
+            # contracts by about this factor per step
+            sk = lu.LUSolver(lu.LUConfig(n, 512, precision=prec))
+            sk.refine_factor(A)
+            try:
+                pn = sk.refine_precond_norm(A, iters=15)
+            except lu.LUError:
+                pn = None
+            del sk
             rows.append({"kappa": kappa, "precision": name, "status": st, "converged": st == 0,
                          "ir_iterations": info["iterations"], "gmres_iterations": info["gmres_iterations"],
-                         "used_gmres": bool(info["used_gmres"]), "r_hpl": r["r_hpl"],
-                         "r_hpl_initial": info["r_hpl_initial"], "forward_error_vs_fp64": fe,
+                         "used_gmres": bool(info["used_gmres"]), "rejected_steps": info["rejected"],
+                         "r_hpl": r["r_hpl"], "r_hpl_initial": info["r_hpl_initial"],
+                         "r_hpl_not_above_initial": r["r_hpl"] <= info["r_hpl_initial"],
+                         "forward_error_vs_fp64": fe, "norm_I_minus_Minv_A": pn,
                          "kappa_eps": kappa * 2.22e-16, "ms": e0.elapsed_time(e1)})
             print(json.dumps(rows[-1]), flush=True)
             del s
@@ -747,6 +759,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-c2", action="store_true")        # skip the N=32768 FP64 sub-record
+    ap.add_argument("--no-fp64", action="store_true")      # mixed mode: skip the FP64 companion run
     ap.add_argument("--no-batched", action="store_true")   # skip the batched sub-record
     ap.add_argument("--workload", default="lu", choices=["lu", "batched", "ksweep", "adjoint", "ooc",
                                                          "blockcyclic", "ooc64"])
@@ -882,7 +895,7 @@ def main():
 
     # FP64 companion (mixed mode): time-to-solution of the FP64 path, same A, b
     fp64 = None
-    if mode == "mixed":
+    if mode == "mixed" and not args.no_fp64:
         step_fp64()
         e = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
         fp64_ms = []

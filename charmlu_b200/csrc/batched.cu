@@ -18,7 +18,8 @@
 //                         swaps applied to the other columns and to b, the
 //                         U row by forward substitution, the trailing update
 //                         in 64 x 128 tiles with 4 x 4 register blocks per
-//                         thread
+//                         thread, the tiles' C and L blocks double-buffered
+//                         in shared memory by async copies
 //   then                  blocked forward / backward substitution
 // On B200 the FP64 SIMT pipe has the same peak as FP64 DMMA, and these
 // per-SM problems are too small for the tensor-core tiles, so FP64 here runs
@@ -88,7 +89,13 @@ __device__ __forceinline__ void tuning_for(int n, int esize, int& nb, int& small
   // shared-memory caps: small path n x (n+1); blocked path panel m x (nb+1) + nb x 128 staging
   const int small_cap = (int)(sqrtf((float)(kBatchSmem / esize)) - 1.f);
   if (small > small_cap) small = small_cap;
-  while (nb > 4 && ((size_t)n * (nb + 1) + (size_t)nb * 128) * esize > kBatchSmem) nb >>= 1;
+  // the update phase reuses the same space: U12 slice, two L and two C tiles
+  while (nb > 4) {
+    const size_t panel_phase = (size_t)n * (nb + 1) + (size_t)nb * 128;
+    const size_t update_phase = (size_t)nb * 128 + (size_t)2 * 64 * nb + (size_t)2 * 64 * 128;
+    if ((panel_phase > update_phase ? panel_phase : update_phase) * esize <= kBatchSmem) break;
+    nb >>= 1;
+  }
 }
 
 template <typename T>
@@ -226,6 +233,110 @@ __device__ void solve_global(const T* LU, int n, T* x, T* s_acc) {
   }
 }
 
+// Element copy global -> shared through the async copy unit; pred false
+// zero-fills the destination (src-size 0: nothing is read).
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(void* sdst, const void* gsrc, bool pred) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(smem_u32(sdst)), "l"(gsrc), "n"(BYTES),
+               "r"(pred ? BYTES : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Trailing update A[c1:n, c1:n] -= L21 * U12 (L21 = A[c1:n, k0:k0+kw], U12 =
+// A[k0:k0+kw, c1:n], both final in global memory) over 64 x 128 tiles, 4 x 4
+// outputs per thread: rows tr*4 .. +3 (one row group per warp: the L reads
+// are broadcasts), columns tc + 32 j (consecutive across lanes: conflict-free
+// shared reads and coalesced global writes).  Per column tile the U12 slice
+// is staged once; the row tiles' C and L blocks stream through two shared
+// buffers with the async copy unit, so the next tile's loads are in flight
+// while this one is computed.  smem (reusing the panel's space):
+//   Ut [nb][128] | Lt[2] [64][nb] | Ct[2] [64][128]
+template <typename T>
+__device__ void trailing_update(T* A, int n, int k0, int kw, int c1, int nb, unsigned char* smem) {
+  const int tid = threadIdx.x, tr = tid >> 5, tc = tid & 31;
+  T* ut = reinterpret_cast<T*>(smem);
+  T* lt = ut + (size_t)nb * 128;
+  T* ctb = lt + 2 * (size_t)64 * nb;
+  const int nrt = (n - c1 + 63) / 64;
+  auto issue = [&](int t, int ct, int buf) {
+    const int rt = c1 + t * 64;
+    T* cdst = ctb + (size_t)buf * 64 * 128;
+    T* ldst = lt + (size_t)buf * 64 * nb;
+    for (int idx = tid; idx < 64 * 128; idx += BT) {
+      const int r = idx >> 7, c = idx & 127;
+      const bool ok = rt + r < n && ct + c < n;
+      cp_async_elem<sizeof(T)>(cdst + idx, ok ? A + (int64_t)(rt + r) * n + ct + c : A, ok);
+    }
+    for (int idx = tid; idx < 64 * nb; idx += BT) {
+      const int r = idx / nb, p = idx - r * nb;
+      const bool ok = rt + r < n && p < kw;
+      cp_async_elem<sizeof(T)>(ldst + idx, ok ? A + (int64_t)(rt + r) * n + k0 + p : A, ok);
+    }
+    cp_async_commit_group();
+  };
+  for (int ct = c1; ct < n; ct += 128) {
+    // U12 slice (kw x 128): all of a thread's loads in flight together
+    for (int base = 0; base < kw * 128; base += BT * 8) {
+      T v[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int idx = base + tid + u * BT;
+        const int p = idx >> 7, c = idx & 127;
+        v[u] = (idx < kw * 128 && ct + c < n) ? A[(int64_t)(k0 + p) * n + ct + c] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int idx = base + tid + u * BT;
+        if (idx < kw * 128) ut[idx] = v[u];
+      }
+    }
+    issue(0, ct, 0);
+    for (int t = 0; t < nrt; t++) {
+      const int buf = t & 1;
+      if (t + 1 < nrt) {
+        issue(t + 1, ct, buf ^ 1);
+        cp_async_wait_group<1>();
+      } else {
+        cp_async_wait_group<0>();
+      }
+      __syncthreads();  // tile t (and, at t = 0, the U12 slice) in shared memory
+      const T* cs = ctb + (size_t)buf * 64 * 128;
+      const T* ls = lt + (size_t)buf * 64 * nb;
+      T acc[4][4];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = cs[(tr * 4 + i) * 128 + tc + 32 * j];
+      for (int p = 0; p < kw; p++) {
+        T av[4], bv[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) av[i] = ls[(tr * 4 + i) * nb + p];
+#pragma unroll
+        for (int j = 0; j < 4; j++) bv[j] = ut[p * 128 + tc + 32 * j];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+          for (int j = 0; j < 4; j++) acc[i][j] = fma(-av[i], bv[j], acc[i][j]);
+      }
+      const int rbase = c1 + t * 64 + tr * 4;
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int r = rbase + i;
+        if (r >= n) break;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int c = ct + tc + 32 * j;
+          if (c < n) A[(int64_t)r * n + c] = acc[i][j];
+        }
+      }
+      __syncthreads();  // buffer `buf` (and the U12 slice after the last tile) free for reuse
+    }
+  }
+}
+
 // Factor A (n x n row-major in global, ld = n) in place, permuting x along
 // with the rows and recording the pivots (global rows) in piv.
 template <typename T>
@@ -254,7 +365,6 @@ __device__ int factor_system(T* A, int n, T* x, int* piv, unsigned char* smem, T
   int info = 0;
   const int ld = nb + 1;
   T* panel = reinterpret_cast<T*>(smem);                  // n x (nb+1)
-  T* ut = panel + (size_t)n * ld;                          // nb x 128
   __shared__ int sw_dst[64], sw_src[64], sw_m;             // composed row moves of a panel
   for (int k0 = 0; k0 < n; k0 += nb) {
     const int kw = min(nb, n - k0), m = n - k0;
@@ -356,67 +466,7 @@ __device__ int factor_system(T* A, int n, T* x, int* piv, unsigned char* smem, T
         if (i < kw) A[(int64_t)(k0 + i) * n + c] = u[i];
     }
     __syncthreads();
-    // trailing update A[c1:n, c1:n] -= L21 * U12 in 64 x 128 tiles, 4 x 4 per
-    // thread: rows tr*4 .. +3 (one row group per warp: the L21 reads are
-    // broadcasts), columns tc + 32 j (consecutive across lanes: conflict-free
-    // shared reads and coalesced global read-modify-writes)
-    const int tr = tid >> 5, tc = tid & 31;
-    for (int ct = c1; ct < n; ct += 128) {
-      // U12 tile (kw x 128): all of a thread's loads in flight together
-      for (int base = 0; base < kw * 128; base += BT * 8) {
-        T v[8];
-#pragma unroll
-        for (int u = 0; u < 8; u++) {
-          const int idx = base + tid + u * BT;
-          const int p = idx >> 7, c = idx & 127;
-          v[u] = (idx < kw * 128 && ct + c < n) ? A[(int64_t)(k0 + p) * n + ct + c] : T(0);
-        }
-#pragma unroll
-        for (int u = 0; u < 8; u++) {
-          const int idx = base + tid + u * BT;
-          if (idx < kw * 128) ut[idx] = v[u];
-        }
-      }
-      __syncthreads();
-      T acc[4][4];
-      auto load_c = [&](int rt, T (&dst)[4][4]) {
-        const int rbase = rt + tr * 4;
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-          for (int j = 0; j < 4; j++) {
-            const int r = rbase + i, c = ct + tc + 32 * j;
-            dst[i][j] = (r < n && c < n) ? A[(int64_t)r * n + c] : T(0);
-          }
-      };
-      load_c(c1, acc);
-      for (int rt = c1; rt < n; rt += 64) {
-        const int rbase = rt + tr * 4;
-        for (int p = 0; p < kw; p++) {
-          T av[4], bv[4];
-#pragma unroll
-          for (int i = 0; i < 4; i++) av[i] = (rbase + i < n) ? panel[(rbase + i - k0) * ld + p] : T(0);
-#pragma unroll
-          for (int j = 0; j < 4; j++) bv[j] = ut[p * 128 + tc + 32 * j];
-#pragma unroll
-          for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 4; j++) acc[i][j] = fma(-av[i], bv[j], acc[i][j]);
-        }
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-          const int r = rbase + i;
-          if (r >= n) break;
-#pragma unroll
-          for (int j = 0; j < 4; j++) {
-            const int c = ct + tc + 32 * j;
-            if (c < n) A[(int64_t)r * n + c] = acc[i][j];
-          }
-        }
-        if (rt + 64 < n) load_c(rt + 64, acc);  // the next row tile's C values
-      }
-      __syncthreads();
-    }
+    trailing_update<T>(A, n, k0, kw, c1, nb, smem);
   }
   return info;
 }
