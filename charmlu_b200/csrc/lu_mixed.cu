@@ -905,7 +905,7 @@ int refine_group(lu_handle h, const double* A, int64_t lda, int trans, const dou
     best_rc[c] = rc[c];
   }
   double worst = worst_of(best_rc);
-  ri->r_hpl_initial = std::max(ri->r_hpl_initial, worst);
+  if (!(worst <= ri->r_hpl_initial)) ri->r_hpl_initial = worst;  // worst over groups (NaN sticks)
   int classical = 0;
   for (int it = 0; std::isfinite(worst) && !(worst < target) && it < max_it; it++) {
     const bool gm_step = gm;

@@ -362,6 +362,10 @@ def test_refinement_never_raises_the_residual(cuda_dev, kappa, prec):
     s = lu.LUSolver(lu.LUConfig(n, 256, precision=prec, ir_max_iter=20, gmres_restart=60))
     x, info = s.refine_solve(A, b)
     st = s.status()
+    if not np.isfinite(info["r_hpl_initial"]):
+        # the low-precision factors broke down (overflow): reported, not refined
+        assert st != 0 and info["status"] != 0, (st, info)
+        return
     assert info["r_hpl"] <= info["r_hpl_initial"], info
     r = s.residual(A, x, b)
     assert abs(r["r_hpl"] - info["r_hpl"]) <= 1e-6 * max(1.0, info["r_hpl"]), (r, info)
@@ -385,6 +389,9 @@ def test_refine_apply_never_raises_the_residual(cuda_dev):
     s.refine_factor(A)
     for trans in (False, True):
         X, info = s.refine_apply(A, B, trans=trans)
+        if not np.isfinite(info["r_hpl_initial"]):
+            assert info["status"] != 0, info
+            continue
         assert info["r_hpl"] <= info["r_hpl_initial"], info
         if info["status"] == 0:
             op = A.t() if trans else A
