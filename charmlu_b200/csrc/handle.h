@@ -63,6 +63,10 @@ struct lu_handle_s {
   // leaf measured best)
   int gemm_ctas = 148, gemm_reserve = 48;
   int gemm_helper = 1;  // look-ahead: reserved SMs join the update once the panel is done
+  // mixed path: FP32 panel leaves of width <= 32 by tournament pivoting
+  // (no grid-wide synchronisation per column); 0 = partial pivoting
+  int tslu = 1;
+  lub::TsluScratch tslu_scr{};
   // FP16x3 mixed path: the recursive FP32 panel's GEMM halves of width >= 128
   // on the tcgen05 kernel, with their own split-operand buffers (the panel
   // runs beside the trailing update, which owns Lb/Ub/amax)

@@ -44,6 +44,24 @@ int launch_getf2_leaf(T* P, int64_t lda, int M, int ncols, int32_t* ipiv, int ro
                       unsigned* bar, DevStatus* st, int info_base, double thr, long long spin, int max_ctas,
                       cudaStream_t s, T* prow0 = nullptr, int pw = 0, int lc0 = 0);
 
+// ---- tournament-pivoting leaf of the FP32 panels (tslu.cu)
+struct TsluScratch {
+  int* cand_idx;      // [kMaxLeafCTAs][kMaxLeafW] rows each block nominates
+  int* cand_cnt;      // [kMaxLeafCTAs]
+  float* lu11;        // [kMaxLeafW][kMaxLeafW] factored top block
+  unsigned* ok_mask;  // [1] bit j: pivot j usable (nonzero, not NaN)
+  int* mv_dst;        // [2 * kMaxLeafW] row moves dst <- src
+  int* mv_src;
+  int* mv_cnt;        // [1]
+  float* mv_data;     // [2 * kMaxLeafW][mv_pitch] moved rows' original values
+  int mv_pitch;       // >= the widest enclosing panel
+};
+int tslu_init();
+// ncols <= 32; LU_ERR_UNSUPPORTED when the shapes exceed its blocks
+int launch_tslu_leaf(float* P, int64_t lda, int M, int ncols, int32_t* ipiv, int row_base, const TsluScratch& scr,
+                     DevStatus* st, int info_base, double thr, int max_ctas, cudaStream_t s, float* prow0, int pw,
+                     int lc0);
+
 // ---- pivot batches: compose sequential swaps into (dst <- src) lists
 // batch: swaps (k0+i) <-> ipiv[k0+i] for i in [0, cnt), cnt <= kMaxBatch
 constexpr int kMaxBatch = 1024;

@@ -69,6 +69,7 @@ int ensure_kernels_init() {
     if (s == LU_OK) s = gemm_bf16_init();
     if (s == LU_OK) s = leaf_init<double>();
     if (s == LU_OK) s = leaf_init<float>();
+    if (s == LU_OK) s = tslu_init();
     return s;
   });
 }
@@ -341,6 +342,7 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
   if (const char* e = getenv("LU_B200_GEMM_HELPER")) h->gemm_helper = atoi(e) != 0;
   if (const char* e = getenv("LU_B200_PANEL_TC")) h->panel_tc = atoi(e) != 0;
   if (const char* e = getenv("LU_B200_LA_SPLIT")) h->la_split = atoi(e) != 0;
+  if (const char* e = getenv("LU_B200_TSLU")) h->tslu = atoi(e) != 0;
   if (const char* e = getenv("LU_B200_STAGE_BYTES")) h->stage_bytes = std::max<size_t>(1 << 16, strtoull(e, nullptr, 10));
   if (const char* e = getenv("LU_B200_RESIDENT_BYTES")) h->resident_cap = strtoull(e, nullptr, 10);
   if (s == LU_OK) s = h->alloc(&h->perm, n);

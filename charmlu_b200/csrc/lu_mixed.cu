@@ -50,6 +50,18 @@ int ensure_mixed(lu_handle h) {
     LUB_TRY(h->alloc(&h->Up, (size_t)B * h->ldkP));
     LUB_TRY(h->alloc(&h->amaxP, 4));
   }
+  if (h->tslu) {
+    TsluScratch& t = h->tslu_scr;
+    t.mv_pitch = (int)B;
+    LUB_TRY(h->alloc(&t.cand_idx, kMaxLeafCTAs * kMaxLeafW));
+    LUB_TRY(h->alloc(&t.cand_cnt, kMaxLeafCTAs));
+    LUB_TRY(h->alloc(&t.lu11, kMaxLeafW * kMaxLeafW));
+    LUB_TRY(h->alloc(&t.ok_mask, 1));
+    LUB_TRY(h->alloc(&t.mv_dst, 2 * kMaxLeafW));
+    LUB_TRY(h->alloc(&t.mv_src, 2 * kMaxLeafW));
+    LUB_TRY(h->alloc(&t.mv_cnt, 1));
+    LUB_TRY(h->alloc(&t.mv_data, (size_t)2 * kMaxLeafW * B));
+  }
   LUB_TRY(h->alloc(&h->v32, n));
   LUB_TRY(h->alloc(&h->r64, n));
   LUB_TRY(h->alloc(&h->z64, n));
@@ -149,9 +161,14 @@ int panel_gemm_tc(Ctx32& c, int r0, int M, int kc, int K, int n0, int N, int cen
 int panel32(Ctx32& c, int c0, int w, int p0, int pw) {
   const int M = c.n - c0;
   if (w <= c.leaf_w) {
+    Prof pf(c.h, c.s, LU_PH_PANEL, (double)M * w * w);
+    if (c.h->tslu && c.h->tslu_scr.cand_idx) {
+      const int rc = launch_tslu_leaf(c.A + (int64_t)c0 * c.ld + c0, c.ld, M, w, c.ipiv + c0, c0, c.h->tslu_scr,
+                                      c.h->st, c0, c.thr, c.leaf_ctas, c.s, c.A + (int64_t)c0 * c.ld + p0, pw, c0 - p0);
+      if (rc != LU_ERR_UNSUPPORTED) return rc;
+    }
     unsigned* bar = c.h->take_counter();
     if (!bar) return LU_ERR_NOMEM;
-    Prof pf(c.h, c.s, LU_PH_PANEL, (double)M * w * w);
     return launch_getf2_leaf<float>(c.A + (int64_t)c0 * c.ld + c0, c.ld, M, w, c.ipiv + c0, c0, c.h->leaf32, bar,
                                     c.h->st, c0, c.thr, c.h->spin, c.leaf_ctas, c.s, c.A + (int64_t)c0 * c.ld + p0,
                                     pw, c0 - p0);
@@ -310,8 +327,10 @@ int factor_mixed(lu_handle h, cudaStream_t s) {
   const int n = (int)h->cfg.n, B = h->cfg.block_size;
   const bool bf16 = h->cfg.precision == LU_PREC_BF16;
   const bool la = h->cfg.lookahead != 0;
+  // the tournament-pivoting leaf handles widths up to 32
+  const int lw = la ? h->leaf_w32_la : h->leaf_w32;
   Ctx32 c{h, h->A32, h->ld32, n, h->ipiv32, s, h->cfg.sing_threshold, h->plist,
-          la ? h->leaf_w32_la : h->leaf_w32, la ? h->leaf_ctas_la : h->leaf_ctas};
+          h->tslu ? std::min(lw, 32) : lw, la ? h->leaf_ctas_la : h->leaf_ctas};
   CUtensorMap mapC;
   LUB_TRY(encode_tmap_2d(&mapC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->A32, n, n, h->ld32 * 4, 32, 128,
                          CU_TENSOR_MAP_SWIZZLE_128B));

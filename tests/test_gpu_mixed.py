@@ -455,3 +455,54 @@ def test_gemm_f32_panel_kernels_match_torch(cuda_dev, M, N, K):
     ref = C0[:, :N].double() - A.double() @ B.double()
     assert (out[0].double() - ref).abs().max().item() <= 4e-7 * K
     assert torch.equal(out[0], out[1])
+
+
+def _tslu(P, ncols, max_ctas=48):
+    from charmlu_b200 import _lib as L
+    f = L.load().lub_test_tslu_leaf
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                  ctypes.c_void_p]
+    f.restype = ctypes.c_int
+    ipiv = torch.zeros(ncols, dtype=torch.int32, device="cuda")
+    rc = f(P.data_ptr(), P.stride(0), P.shape[0], ncols, ipiv.data_ptr(), max_ctas,
+           torch.cuda.current_stream().cuda_stream)
+    return rc, ipiv
+
+
+@pytest.mark.parametrize("M,ncols,max_ctas", [(65536, 32, 48), (5000, 32, 48), (3001, 17, 48), (100, 8, 48),
+                                              (32, 32, 48), (20000, 16, 8), (70000, 32, 148)])
+def test_tslu_leaf_factors_the_permuted_panel(cuda_dev, M, ncols, max_ctas):
+    """The tournament-pivoting leaf: its sequential swaps applied to the
+    original panel give P A = L U (FP32, checked in FP64), every pivot lies
+    in [j, M), the first pivot is the column's largest entry (lowest row on
+    a tie), and the multipliers stay bounded."""
+    g = torch.Generator(device="cuda").manual_seed(M + ncols)
+    A = torch.rand(M, ncols + 3, device="cuda", generator=g)[:, :ncols] - 0.5
+    A0 = A.double().cpu().numpy()
+    P = A.clone()
+    Pv = P[:, :ncols]
+    rc, ipiv = _tslu(Pv, ncols, max_ctas)
+    assert rc == 0, rc
+    ip = ipiv.cpu().numpy()
+    assert all(j <= ip[j] < M for j in range(ncols)), ip
+    col = np.abs(A0[:, 0])
+    assert ip[0] == int(np.flatnonzero(col == col.max())[0])
+    PA = A0.copy()
+    for j, p in enumerate(ip):
+        PA[[j, p]] = PA[[p, j]]
+    LU = Pv.double().cpu().numpy()
+    Lm = np.tril(LU, -1)[:, :ncols]
+    Lm[:ncols, :ncols] += np.eye(ncols)
+    U = np.triu(LU[:ncols])
+    err = np.abs(PA - Lm @ U).max() / np.abs(A0).max()
+    assert err < 2e-6 * ncols, err
+    assert np.abs(Lm).max() < 50.0
+
+
+def test_tslu_leaf_reports_a_zero_column(cuda_dev):
+    M, ncols = 4096, 32
+    g = torch.Generator(device="cuda").manual_seed(5)
+    A = torch.rand(M, ncols, device="cuda", generator=g) - 0.5
+    A[:, 9] = 0.0
+    rc, ipiv = _tslu(A, ncols)
+    assert rc == 10, rc
