@@ -48,6 +48,8 @@ int launch_getf2_leaf(T* P, int64_t lda, int M, int ncols, int32_t* ipiv, int ro
 struct TsluScratch {
   int* cand_idx;      // [kMaxLeafCTAs][kMaxLeafW] rows each block nominates
   int* cand_cnt;      // [kMaxLeafCTAs]
+  int* cand_idx2;     // the same, for the tournament's alternate rounds
+  int* cand_cnt2;
   float* lu11;        // [kMaxLeafW][kMaxLeafW] factored top block
   unsigned* ok_mask;  // [1] bit j: pivot j usable (nonzero, not NaN)
   int* mv_dst;        // [2 * kMaxLeafW] row moves dst <- src

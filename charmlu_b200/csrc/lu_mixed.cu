@@ -55,6 +55,8 @@ int ensure_mixed(lu_handle h) {
     t.mv_pitch = (int)B;
     LUB_TRY(h->alloc(&t.cand_idx, kMaxLeafCTAs * kMaxLeafW));
     LUB_TRY(h->alloc(&t.cand_cnt, kMaxLeafCTAs));
+    LUB_TRY(h->alloc(&t.cand_idx2, kMaxLeafCTAs * kMaxLeafW));
+    LUB_TRY(h->alloc(&t.cand_cnt2, kMaxLeafCTAs));
     LUB_TRY(h->alloc(&t.lu11, kMaxLeafW * kMaxLeafW));
     LUB_TRY(h->alloc(&t.ok_mask, 1));
     LUB_TRY(h->alloc(&t.mv_dst, 2 * kMaxLeafW));

@@ -470,7 +470,7 @@ def _tslu(P, ncols, max_ctas=48):
 
 
 @pytest.mark.parametrize("M,ncols,max_ctas", [(65536, 32, 48), (5000, 32, 48), (3001, 17, 48), (100, 8, 48),
-                                              (32, 32, 48), (20000, 16, 8), (70000, 32, 148)])
+                                              (32, 32, 48), (20000, 16, 8), (60000, 32, 148)])
 def test_tslu_leaf_factors_the_permuted_panel(cuda_dev, M, ncols, max_ctas):
     """The tournament-pivoting leaf: its sequential swaps applied to the
     original panel give P A = L U (FP32, checked in FP64), every pivot lies
@@ -497,6 +497,17 @@ def test_tslu_leaf_factors_the_permuted_panel(cuda_dev, M, ncols, max_ctas):
     err = np.abs(PA - Lm @ U).max() / np.abs(A0).max()
     assert err < 2e-6 * ncols, err
     assert np.abs(Lm).max() < 50.0
+
+
+def test_tslu_leaf_declines_panels_beyond_its_blocks(cuda_dev):
+    """A panel taller than the row blocks and the stack can hold is left
+    untouched and declined (LU_ERR_UNSUPPORTED): the caller then runs the
+    partial-pivoting leaf."""
+    M, ncols = 80000, 32
+    A = torch.rand(M, ncols, device="cuda") - 0.5
+    A0 = A.clone()
+    rc, _ = _tslu(A, ncols)
+    assert rc == -8 and torch.equal(A, A0)
 
 
 def test_tslu_leaf_reports_a_zero_column(cuda_dev):
