@@ -64,8 +64,10 @@ struct lu_handle_s {
   int gemm_ctas = 148, gemm_reserve = 48;
   int gemm_helper = 1;  // look-ahead: reserved SMs join the update once the panel is done
   // mixed path: FP32 panel leaves of width <= 32 by tournament pivoting
-  // (no grid-wide synchronisation per column); 0 = partial pivoting
-  int tslu = 1;
+  // (no grid-wide synchronisation per column) when 1; partial pivoting by
+  // default (LU_B200_TSLU=1 selects the tournament: about as fast, see
+  // tslu.cu, and its refinement contraction varies with the row blocks)
+  int tslu = 0;
   lub::TsluScratch tslu_scr{};
   // FP16x3 mixed path: the recursive FP32 panel's GEMM halves of width >= 128
   // on the tcgen05 kernel, with their own split-operand buffers (the panel

@@ -50,7 +50,7 @@ int ensure_mixed(lu_handle h) {
     LUB_TRY(h->alloc(&h->Up, (size_t)B * h->ldkP));
     LUB_TRY(h->alloc(&h->amaxP, 4));
   }
-  if (h->tslu) {
+  if (h->tslu && !h->tslu_scr.cand_idx) {
     TsluScratch& t = h->tslu_scr;
     t.mv_pitch = (int)B;
     LUB_TRY(h->alloc(&t.cand_idx, kMaxLeafCTAs * kMaxLeafW));

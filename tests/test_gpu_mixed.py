@@ -517,3 +517,15 @@ def test_tslu_leaf_reports_a_zero_column(cuda_dev):
     A[:, 9] = 0.0
     rc, ipiv = _tslu(A, ncols)
     assert rc == 10, rc
+
+
+@pytest.mark.parametrize("n,b,la", [(4096, 512, True), (3000, 256, True), (2048, 256, False)])
+def test_refine_solve_with_tournament_leaf(cuda_dev, n, b, la, monkeypatch):
+    """LU_B200_TSLU=1: the mixed factorisation with the tournament-pivoting
+    leaf meets the residual contract and the forward-error bar."""
+    monkeypatch.setenv("LU_B200_TSLU", "1")
+    s, A, rhs, x, info, st = _refine(n, b, prec=3, lookahead=la)
+    assert st == 0 and info["status"] == 0, info
+    assert s.residual(A, x, rhs)["r_hpl"] < 16
+    x_ref, *_ = oracle.solve(A.cpu().numpy(), rhs.cpu().numpy(), b=128)
+    assert np.abs(x.cpu().numpy() - x_ref).max() / np.abs(x_ref).max() < 1e-6
