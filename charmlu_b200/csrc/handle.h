@@ -68,6 +68,9 @@ struct lu_handle_s {
   // default (LU_B200_TSLU=1 selects the tournament: about as fast, see
   // tslu.cu, and its refinement contraction varies with the row blocks)
   int tslu = 0;
+  // mixed path: the panels' inner TRSMs (w <= 256) as one blocked launch
+  // instead of the recursion (LU_B200_TRSM_BLOCK=0 restores the recursion)
+  int trsm_block = 1;
   lub::TsluScratch tslu_scr{};
   // FP16x3 mixed path: the recursive FP32 panel's GEMM halves of width >= 128
   // on the tcgen05 kernel, with their own split-operand buffers (the panel

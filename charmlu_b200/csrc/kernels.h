@@ -92,6 +92,8 @@ int launch_ipiv_to_perm(const int32_t* ipiv, int n, int32_t* perm, int32_t* work
 // B(m x ncols) <- L^{-1} B, L unit lower m x m (m <= 32), row-major
 template <typename T>
 int launch_trsm_llu_leaf(const T* L, int64_t ldl, T* B, int64_t ldb, int m, int ncols, cudaStream_t s);
+// FP32 B(w x ncols) <- L^{-1} B, L unit lower w x w, w <= 256, one launch
+int launch_trsm_llu_block(const float* L, int64_t ldl, float* B, int64_t ldb, int w, int ncols, cudaStream_t s);
 // single/multi right-hand side substitution with flags (persistent tickets)
 template <typename T>
 int launch_trsv(const T* LU, int64_t lda, int n, T* x, int upper, int* flags, unsigned* ticket, DevStatus* st,

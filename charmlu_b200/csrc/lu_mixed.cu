@@ -122,6 +122,11 @@ int sgemm(Ctx32& c, int rc, int cc, int ra, int ca, int rb, int cb, int M, int N
 }
 
 int trsm32(Ctx32& c, int r0, int w, int rb, int cb, int ncols) {
+  if (w > 32 && w <= 256 && ncols <= 512 && c.h->trsm_block) {  // the panels' inner solves: one launch
+    Prof pf(c.h, c.s, LU_PH_TRSM, (double)w * w * ncols);
+    return launch_trsm_llu_block(c.A + (int64_t)r0 * c.ld + r0, c.ld, c.A + (int64_t)rb * c.ld + cb, c.ld, w, ncols,
+                                 c.s);
+  }
   if (w <= 32) {
     Prof pf(c.h, c.s, LU_PH_TRSM, (double)w * w * ncols);
     return launch_trsm_llu_leaf<float>(c.A + (int64_t)r0 * c.ld + r0, c.ld, c.A + (int64_t)rb * c.ld + cb, c.ld, w,

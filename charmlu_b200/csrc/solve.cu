@@ -48,6 +48,76 @@ __global__ void __launch_bounds__(128) trsm_llu_leaf_kernel(const T* L, int64_t 
     if (i < m) B[(int64_t)i * ldb + col] = x[i];
 }
 
+// B (w x ncols) <- L^{-1} B, L unit lower w x w (w <= kTrsmBlockMaxW), FP32,
+// in one launch: each CTA keeps a 32-column slice of B in shared memory and
+// walks down L in 32-row blocks, solving the block's diagonal part (one
+// thread per column, in registers) and then updating the rows below it with
+// the block's columns of L.  This replaces the recursion's chain of small
+// launches (for w = 256: 8 leaf solves and 7 GEMMs) inside the mixed path's
+// panels.
+constexpr int kTrsmBlockMaxW = 256;
+constexpr int kTrsmCB = 32;   // columns of B per CTA
+constexpr int kTrsmNT = 256;
+
+__global__ void __launch_bounds__(kTrsmNT) trsm_llu_block_kernel(const float* __restrict__ L, int64_t ldl,
+                                                                 float* __restrict__ B, int64_t ldb, int w,
+                                                                 int ncols) {
+  __shared__ float sB[kTrsmBlockMaxW][kTrsmCB + 1];
+  __shared__ float sL[32][33];
+  const int tid = threadIdx.x;
+  const int c0 = blockIdx.x * kTrsmCB;
+  const int nc = min(kTrsmCB, ncols - c0);
+  for (int idx = tid; idx < w * kTrsmCB; idx += kTrsmNT) {
+    const int r = idx / kTrsmCB, c = idx - r * kTrsmCB;
+    sB[r][c] = c < nc ? B[(int64_t)r * ldb + c0 + c] : 0.f;
+  }
+  for (int k0 = 0; k0 < w; k0 += 32) {
+    const int kb = min(32, w - k0);
+    for (int idx = tid; idx < 32 * 32; idx += kTrsmNT) {
+      const int i = idx >> 5, p = idx & 31;
+      sL[i][p] = (i < kb && p < i) ? L[(int64_t)(k0 + i) * ldl + k0 + p] : 0.f;
+    }
+    __syncthreads();
+    // the diagonal block: forward substitution down each column
+    if (tid < kTrsmCB) {
+      float x[32];
+#pragma unroll
+      for (int i = 0; i < 32; i++) x[i] = i < kb ? sB[k0 + i][tid] : 0.f;
+#pragma unroll
+      for (int i = 1; i < 32; i++) {
+#pragma unroll
+        for (int p = 0; p < i; p++) x[i] = fmaf(-sL[i][p], x[p], x[i]);
+      }
+#pragma unroll
+      for (int i = 0; i < 32; i++)
+        if (i < kb) sB[k0 + i][tid] = x[i];
+    }
+    __syncthreads();
+    // the rows below: B[r, :] -= L[r, k0:k0+kb] B[k0:k0+kb, :], 4 columns per thread
+    const int tx = tid & 7, ty = tid >> 3;
+    for (int r = k0 + kb + ty; r < w; r += kTrsmNT / 8) {
+      const float* lr = L + (int64_t)r * ldl + k0;
+      float a0 = sB[r][4 * tx], a1 = sB[r][4 * tx + 1], a2 = sB[r][4 * tx + 2], a3 = sB[r][4 * tx + 3];
+      for (int p = 0; p < kb; p++) {
+        const float l = __ldg(&lr[p]);
+        a0 = fmaf(-l, sB[k0 + p][4 * tx], a0);
+        a1 = fmaf(-l, sB[k0 + p][4 * tx + 1], a1);
+        a2 = fmaf(-l, sB[k0 + p][4 * tx + 2], a2);
+        a3 = fmaf(-l, sB[k0 + p][4 * tx + 3], a3);
+      }
+      sB[r][4 * tx] = a0;
+      sB[r][4 * tx + 1] = a1;
+      sB[r][4 * tx + 2] = a2;
+      sB[r][4 * tx + 3] = a3;
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < w * kTrsmCB; idx += kTrsmNT) {
+    const int r = idx / kTrsmCB, c = idx - r * kTrsmCB;
+    if (c < nc) B[(int64_t)r * ldb + c0 + c] = sB[r][c];
+  }
+}
+
 constexpr int TB = 64;  // rows per TRSV block
 
 // Inverse of the diagonal tile, computed by each pipeline CTA before it
@@ -514,6 +584,14 @@ int launch_trsm_llu_leaf(const T* L, int64_t ldl, T* B, int64_t ldb, int m, int 
   return LU_OK;
 }
 
+int launch_trsm_llu_block(const float* L, int64_t ldl, float* B, int64_t ldb, int w, int ncols, cudaStream_t s) {
+  if (w <= 1 || ncols <= 0) return LU_OK;
+  if (w > kTrsmBlockMaxW) return LU_ERR_ARG;
+  trsm_llu_block_kernel<<<ceil_div(ncols, kTrsmCB), kTrsmNT, 0, s>>>(L, ldl, B, ldb, w, ncols);
+  LUB_LAUNCH_CHECK();
+  return LU_OK;
+}
+
 template <typename TS, typename T>
 int launch_trsv_mixed(const TS* LU, int64_t lda, int n, T* x, int upper, int* flags, unsigned* ticket, DevStatus* st,
                       long long spin, cudaStream_t s) {
@@ -595,3 +673,8 @@ extern "C" __attribute__((visibility("default"))) int lub_test_wait_timeout(long
   return rc;
 }
 
+// Test hook (not part of the ABI): the blocked FP32 TRSM B <- L^{-1} B.
+extern "C" __attribute__((visibility("default"))) int lub_test_trsm_block(const float* L, int64_t ldl, float* B,
+                                                                        int64_t ldb, int w, int ncols, void* stream) {
+  return lub::launch_trsm_llu_block(L, ldl, B, ldb, w, ncols, (cudaStream_t)stream);
+}

@@ -529,3 +529,26 @@ def test_refine_solve_with_tournament_leaf(cuda_dev, n, b, la, monkeypatch):
     assert s.residual(A, x, rhs)["r_hpl"] < 16
     x_ref, *_ = oracle.solve(A.cpu().numpy(), rhs.cpu().numpy(), b=128)
     assert np.abs(x.cpu().numpy() - x_ref).max() / np.abs(x_ref).max() < 1e-6
+
+
+@pytest.mark.parametrize("w,ncols", [(256, 256), (256, 512), (160, 96), (33, 5), (64, 64), (200, 37)])
+def test_trsm_block_matches_torch(cuda_dev, w, ncols):
+    """The one-launch blocked FP32 TRSM of the mixed path's panels (B <-
+    L^{-1} B, L unit lower) against a plain FP32 torch triangular solve."""
+    from charmlu_b200 import _lib as L
+    f = L.load().lub_test_trsm_block
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
+                  ctypes.c_void_p]
+    f.restype = ctypes.c_int
+    g = torch.Generator(device="cuda").manual_seed(w + ncols)
+    Lm = (torch.rand(w, w + 2, device="cuda", generator=g) - 0.5)[:, :w] * 0.2
+    B = torch.rand(w, ncols + 3, device="cuda", generator=g) - 0.5
+    B0 = B.clone()
+    Bv = B[:, :ncols]
+    assert f(Lm.data_ptr(), Lm.stride(0), Bv.data_ptr(), B.stride(0), w, ncols,
+             torch.cuda.current_stream().cuda_stream) == 0
+    torch.cuda.synchronize()
+    Lu = torch.tril(Lm, -1) + torch.eye(w, device="cuda")
+    ref = torch.linalg.solve_triangular(Lu, B0[:, :ncols], upper=False, unitriangular=True)
+    assert torch.equal(B[:, ncols:], B0[:, ncols:])
+    assert (Bv - ref).abs().max().item() <= 1e-5 * max(1.0, ref.abs().max().item())
