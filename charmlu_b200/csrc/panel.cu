@@ -32,14 +32,6 @@
 namespace lub {
 namespace {
 
-// Columns are eliminated in groups of KG: a rank-1 update touches only the
-// rest of the current group, the columns past the group get one delayed
-// rank-KG update when the group ends, and a row that becomes a pivot row is
-// first brought up to date from the group's earlier pivot rows.  Every
-// element still sees the same FMAs in the same order as with immediate
-// rank-1 updates (bitwise the same factors), with about a third of the
-// shared-memory traffic.
-constexpr int KG = 8;
 
 template <typename T>
 __device__ __forceinline__ bool cand_better(T v1, int r1, T v2, int r2) {
@@ -58,26 +50,6 @@ __device__ __forceinline__ void warp_argmax(T& v, int& r, int& w) {
   }
 }
 
-// s_v, s_r: NT/32 + 1 entries
-template <typename T, int NT>
-__device__ __forceinline__ void block_argmax(T v, int r, T* s_v, int* s_r, T& out_v, int& out_r) {
-  constexpr int NW = NT / 32;
-  int w = 0;
-  warp_argmax(v, r, w);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) { s_v[warp] = v; s_r[warp] = r; }
-  __syncthreads();
-  if (warp == 0) {
-    v = lane < NW ? s_v[lane] : T(0);
-    r = lane < NW ? s_r[lane] : -1;
-    warp_argmax(v, r, w);
-    if (lane == 0) { s_v[NW] = v; s_r[NW] = r; }
-  }
-  __syncthreads();
-  out_v = s_v[NW];
-  out_r = s_r[NW];
-}
-
 // Candidate rows read speculatively per thread after the barrier (G * W
 // values spread over the CTA); above this many per thread the pivot row is
 // read after the argmax instead (a second round trip).
@@ -92,17 +64,15 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
   // then arithmetic, then stores), so their shared-memory round trips and
   // divisions overlap: fewer when more threads share the rows
   constexpr int RU = NT >= 1024 ? 1 : (NT >= 512 ? 2 : 4);
+  constexpr int NW = NT / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int LD = W + 1;
   T* a = reinterpret_cast<T*>(smem_raw);  // [R][LD]
   T* urow = a + (size_t)R * LD;           // [W] pivot row
-  __shared__ T s_v[NT / 32 + 1];
-  __shared__ int s_r[NT / 32 + 1];
-  __shared__ int s_p, s_win;
-  __shared__ T uhist[KG][W];     // pivot rows of the current group
-  __shared__ unsigned s_scaled;  // group columns whose pivot was usable
+  __shared__ T s_v[NW];
+  __shared__ int s_r[NW];
 
-  const int G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x;
+  const int G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r_lo = cta * R;
   const int r_hi = min(M, r_lo + R);
   const int nr = r_hi - r_lo;
@@ -112,6 +82,20 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
     a[r * LD + c] = P[(int64_t)(r_lo + r) * lda + c];
   }
   __syncthreads();
+
+  // every warp reduces the NW per-warp candidates in s_v / s_r itself, so
+  // the whole CTA knows the result after one barrier
+  auto cta_argmax = [&](T bv, int br, T& out_v, int& out_r) {
+    int w = 0;
+    warp_argmax(bv, br, w);
+    if (lane == 0) { s_v[warp] = bv; s_r[warp] = br; }
+    __syncthreads();
+    T v = lane < NW ? s_v[lane] : T(0);
+    int r = lane < NW ? s_r[lane] : -1;
+    warp_argmax(v, r, w);
+    out_v = v;
+    out_r = r;
+  };
 
   // candidate of column 0 (findMaxElm(0, 0), lu.ci:266)
   T cv = 0;
@@ -123,12 +107,13 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
       T v = fabs(a[r * LD]);
       if (v > bv) { bv = v; br = r_lo + r; }
     }
-    block_argmax<T, NT>(bv, br, s_v, s_r, cv, cr);
+    cta_argmax(bv, br, cv, cr);
   }
 
   for (int j = 0; j < ncols; j++) {
     const int slot = j & 1;
-    // ---- publish candidate, its row, and row j if owned
+    // ---- publish the candidate, its row, and row j if owned (every row
+    //      already holds all of the earlier columns' updates)
     if (tid < ncols) {
       if (cr >= 0) scr.cand_data[((size_t)slot * kMaxLeafCTAs + cta) * kMaxLeafW + tid] = a[(cr - r_lo) * LD + tid];
       if (j >= r_lo && j < r_hi) scr.rowj[slot * kMaxLeafW + tid] = a[(j - r_lo) * LD + tid];
@@ -141,8 +126,9 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
     // these writes visible to every CTA that passes the barrier
     if (!grid_barrier(bar, (unsigned)(j + 1) * (unsigned)G, st, spin, 201)) return;
 
-    // ---- global argmax over the G candidates; meanwhile the other threads
-    //      read every candidate row (and row j) from the same round trip
+    // ---- one round trip to L2: every warp reads the G candidate values and
+    //      reduces them (each warp knows the winner without a barrier), and
+    //      every candidate row and row j are read into registers meanwhile
     const bool spec = G * ncols <= kSpecPerThread * NT;
     T sv[kSpecPerThread];
     int sq[kSpecPerThread];
@@ -160,47 +146,28 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
       }
     }
     if (tid < ncols) rj = __ldcg(&scr.rowj[slot * kMaxLeafW + tid]);
-    if (tid < 32) {
+    int pwin = -1, win = 0;
+    {
       T v = 0;
-      int r = -1, w = 0;
-      for (int q = tid; q < G; q += 32) {
-        T v2 = __ldcg(&scr.cand_val[slot * kMaxLeafCTAs + q]);
-        int r2 = __ldcg(&scr.cand_row[slot * kMaxLeafCTAs + q]);
-        if (cand_better(v2, r2, v, r)) { v = v2; r = r2; w = q; }
+      int r = -1;
+      for (int q = lane; q < G; q += 32) {
+        const T v2 = __ldcg(&scr.cand_val[slot * kMaxLeafCTAs + q]);
+        const int r2 = __ldcg(&scr.cand_row[slot * kMaxLeafCTAs + q]);
+        if (cand_better(v2, r2, v, r)) { v = v2; r = r2; win = q; }
       }
-      warp_argmax(v, r, w);
-      if (tid == 0) { s_p = r; s_win = w; }
+      warp_argmax(v, r, win);
+      pwin = r;
     }
-    __syncthreads();
-    const bool zero_col = s_p < 0;
-    const int p = zero_col ? j : s_p;
+    const bool zero_col = pwin < 0;
+    const int p = zero_col ? j : pwin;
     if (zero_col) {
       if (tid < ncols) urow[tid] = rj;
     } else if (spec) {
 #pragma unroll
       for (int e = 0; e < kSpecPerThread; e++)
-        if (sq[e] == s_win) urow[tid + e * NT - s_win * ncols] = sv[e];
+        if (sq[e] == win) urow[tid + e * NT - win * ncols] = sv[e];
     } else if (tid < ncols) {
-      urow[tid] = __ldcg(&scr.cand_data[((size_t)slot * kMaxLeafCTAs + s_win) * kMaxLeafW + tid]);
-    }
-    __syncthreads();
-    // the pivot row's columns past the group still lack the group's earlier
-    // rank-1 updates (its multipliers are urow[g0 .. j))
-    const int g0 = (j / KG) * KG, g1 = min(ncols, g0 + KG);
-    if (j > g0) {
-      const unsigned mask = s_scaled;
-      if (tid >= g1 && tid < ncols) {
-        T v = urow[tid];
-        for (int t = g0; t < j; t++)
-          if ((mask >> (t - g0)) & 1u) v = fma(-urow[t], uhist[t - g0][tid], v);
-        urow[tid] = v;
-      }
-      __syncthreads();
-    }
-    if (tid < ncols) {
-      if (p != j && p >= r_lo && p < r_hi) a[(p - r_lo) * LD + tid] = rj;
-      // position j takes the (brought up to date) pivot row, also when p == j
-      if (j >= r_lo && j < r_hi) a[(j - r_lo) * LD + tid] = urow[tid];
+      urow[tid] = __ldcg(&scr.cand_data[((size_t)slot * kMaxLeafCTAs + win) * kMaxLeafW + tid]);
     }
     // the swap on the enclosing panel's other columns (prow0: panel's first
     // column in this leaf's top row, pw columns, the leaf at lc0): each CTA a
@@ -218,25 +185,27 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
         r2[col] = t;
       }
     }
+    __syncthreads();  // urow complete
+    // ---- the local swap: row p takes the old row j, row j the pivot row
+    if (tid < ncols) {
+      if (p != j && p >= r_lo && p < r_hi) a[(p - r_lo) * LD + tid] = rj;
+      if (j >= r_lo && j < r_hi) a[(j - r_lo) * LD + tid] = urow[tid];
+    }
     const T piv = urow[j];
     if (cta == 0 && tid == 0) {
       ipiv[j] = row_base + p;
       if (!(fabs((double)piv) > thr)) dev_singular(st, info_base + j + 1);
     }
-    const bool do_scale = (piv != T(0)) && !isnan(piv);
-    if (tid < ncols) uhist[j - g0][tid] = urow[tid];
-    if (tid == 0) s_scaled = (j == g0 ? 0u : s_scaled) | (do_scale ? (1u << (j - g0)) : 0u);
-    __syncthreads();
+    __syncthreads();  // rows j and p in place
 
-    // ---- multipliers, rank-1 update of the remaining leaf columns, and the
-    //      candidate of column j+1 in the same pass
+    // ---- multipliers (true division), rank-1 update of the leaf's
+    //      remaining columns, and the candidate of column j+1, in one pass
+    const bool do_scale = (piv != T(0)) && !isnan(piv);
     const bool has_next = j + 1 < ncols;
-    const bool delay = (j == g1 - 1) && (g1 < ncols);
-    const unsigned gmask = s_scaled;
     T bv = 0;
     int br = -1;
     const int r_first = max(j + 1 - r_lo, 0);
-    // pivot-row values are warp-wide broadcasts; RU rows per thread at once
+    // pivot-row values are warp-wide broadcasts
     for (int rb = r_first + tid; rb < nr; rb += NT * RU) {
       T* rp[RU];
       bool live[RU];
@@ -255,37 +224,13 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
 #pragma unroll
         for (int u = 0; u < RU; u++)
           if (live[u]) rp[u][j] = l[u];
-        for (int c = j + 1; c < g1; c++) {
+        for (int c = j + 1; c < ncols; c++) {
           const T uc = urow[c];
           T v[RU];
 #pragma unroll
           for (int u = 0; u < RU; u++) v[u] = live[u] ? rp[u][c] : T(0);
 #pragma unroll
           for (int u = 0; u < RU; u++) v[u] = fma(-l[u], uc, v[u]);
-#pragma unroll
-          for (int u = 0; u < RU; u++)
-            if (live[u]) rp[u][c] = v[u];
-        }
-      }
-      if (delay) {  // the group's rank-KG update of the columns past it
-        T lv[RU][KG];
-#pragma unroll
-        for (int u = 0; u < RU; u++)
-#pragma unroll
-          for (int t = 0; t < KG; t++)
-            lv[u][t] = (live[u] && g0 + t < g1 && ((gmask >> t) & 1u)) ? rp[u][g0 + t] : T(0);
-        for (int c = g1; c < ncols; c++) {
-          T v[RU];
-#pragma unroll
-          for (int u = 0; u < RU; u++) v[u] = live[u] ? rp[u][c] : T(0);
-#pragma unroll
-          for (int t = 0; t < KG; t++) {
-            if (g0 + t < g1 && ((gmask >> t) & 1u)) {
-              const T uh = uhist[t][c];
-#pragma unroll
-              for (int u = 0; u < RU; u++) v[u] = fma(-lv[u][t], uh, v[u]);
-            }
-          }
 #pragma unroll
           for (int u = 0; u < RU; u++)
             if (live[u]) rp[u][c] = v[u];
@@ -301,7 +246,9 @@ getf2_leaf_kernel(T* P, int64_t lda, int M, int ncols, int R, int32_t* ipiv, int
         }
       }
     }
-    block_argmax<T, NT>(bv, br, s_v, s_r, cv, cr);
+    cta_argmax(bv, br, cv, cr);
+    // the barrier inside cta_argmax also ends every thread's update, so the
+    // candidate row published next is complete
   }
 
   for (int idx = tid; idx < nr * ncols; idx += NT) {
