@@ -63,6 +63,7 @@ struct lu_handle_s {
   // leaf measured best)
   int gemm_ctas = 148, gemm_reserve = 48;
   int gemm_helper = 1;  // look-ahead: reserved SMs join the update once the panel is done
+  int gemm_pair = 1;    // pairs layout on CTA pairs (tcgen05 cta_group::2, 256 x 256 tiles)
   // mixed path: FP32 panel leaves of width <= 32 by tournament pivoting
   // (no grid-wide synchronisation per column) when 1; partial pivoting by
   // default (LU_B200_TSLU=1 selects the tournament: about as fast, see

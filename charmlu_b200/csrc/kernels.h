@@ -171,7 +171,7 @@ int launch_gemm_bf16_tc(const CUtensorMap& mapA, const CUtensorMap& mapB, const 
 int launch_gemm_lowp_persistent(const CUtensorMap& mapA, const CUtensorMap& mapB, const CUtensorMap& mapC,
                                 int a_row0, int b_row0, int c_row0, int c_col0, int M, int N, int K, bool bf16,
                                 const unsigned* amax, DevStatus* st, long long spin, int max_ctas, cudaStream_t s,
-                                int kpart = 0, unsigned* tile_ctr = nullptr);
+                                int kpart = 0, unsigned* tile_ctr = nullptr, bool cta_pair = false);
 // |max| of the L21 (rows x K) and U12 (K x N) FP32 panels into amax[0], amax[1]
 int launch_panel_absmax(const float* L, int64_t ldl, int rows, int K, const float* U, int64_t ldu, int N,
                         unsigned* amax, cudaStream_t s);

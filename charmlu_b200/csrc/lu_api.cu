@@ -340,6 +340,7 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
   if (const char* e = getenv("LU_B200_GEMM_CTAS")) h->gemm_ctas = std::max(0, atoi(e));
   if (const char* e = getenv("LU_B200_GEMM_RESERVE")) h->gemm_reserve = std::max(0, atoi(e));
   if (const char* e = getenv("LU_B200_GEMM_HELPER")) h->gemm_helper = atoi(e) != 0;
+  if (const char* e = getenv("LU_B200_GEMM_PAIR")) h->gemm_pair = atoi(e) != 0;
   if (const char* e = getenv("LU_B200_PANEL_TC")) h->panel_tc = atoi(e) != 0;
   if (const char* e = getenv("LU_B200_LA_SPLIT")) h->la_split = atoi(e) != 0;
   if (const char* e = getenv("LU_B200_TSLU")) h->tslu = atoi(e) != 0;

@@ -154,13 +154,13 @@ int panel_gemm_tc(Ctx32& c, int r0, int M, int kc, int K, int n0, int N, int cen
   CUtensorMap mL, mU, mC;
   LUB_TRY(encode_tmap_2d(&mL, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, h->Lp, 2 * K, M, h->ldkP * 2, 64, 128,
                          CU_TENSOR_MAP_SWIZZLE_128B));
-  LUB_TRY(encode_tmap_2d(&mU, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, h->Up, 2 * K, N, h->ldkP * 2, 64, 256,
+  LUB_TRY(encode_tmap_2d(&mU, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, h->Up, 2 * K, N, h->ldkP * 2, 64, 128,
                          CU_TENSOR_MAP_SWIZZLE_128B));
   LUB_TRY(encode_tmap_2d(&mC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, c.A, cend, c.n, c.ld * 4, 32, 128,
                          CU_TENSOR_MAP_SWIZZLE_128B));
   const int ctas = h->cfg.lookahead ? h->gemm_reserve : h->gemm_ctas;
   return launch_gemm_lowp_persistent(mL, mU, mC, 0, 0, r0, n0, M, N, K, false, h->amaxP, h->st, h->spin,
-                                     std::max(1, ctas), c.s, K);
+                                     std::max(1, ctas), c.s, K, nullptr, h->gemm_pair != 0);
 }
 
 // recursive FP32 panel of columns [c0, c0+w) inside the panel [p0, p0+pw);
@@ -226,7 +226,7 @@ int build_operands(lu_handle h, const Ctx32& c, int k0, int kw, int k1, int rest
   }
   const CUtensorMapDataType dt = bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
   LUB_TRY(encode_tmap_2d(mapL, dt, 2, h->Lb, ke, rest, h->ldk * 2, 64, 128, CU_TENSOR_MAP_SWIZZLE_128B));
-  LUB_TRY(encode_tmap_2d(mapU, dt, 2, h->Ub, ke, rest, h->ldk * 2, 64, 256, CU_TENSOR_MAP_SWIZZLE_128B));
+  LUB_TRY(encode_tmap_2d(mapU, dt, 2, h->Ub, ke, rest, h->ldk * 2, 64, 128, CU_TENSOR_MAP_SWIZZLE_128B));
   return LU_OK;
 }
 
@@ -255,7 +255,7 @@ int build_operands_part(lu_handle h, const Ctx32& c, int k0, int kw, int k1, int
   }
   LUB_TRY(encode_tmap_2d(mapL, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, h->Lb, 2 * kps, rest, h->ldk * 2, 64, 128,
                          CU_TENSOR_MAP_SWIZZLE_128B));
-  return encode_tmap_2d(mapU, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, h->Ub, 2 * kps, rest, h->ldk * 2, 64, 256,
+  return encode_tmap_2d(mapU, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, h->Ub, 2 * kps, rest, h->ldk * 2, 64, 128,
                         CU_TENSOR_MAP_SWIZZLE_128B);
 }
 
@@ -270,14 +270,16 @@ int lowp_gemm(lu_handle h, const CUtensorMap& mapL, const CUtensorMap& mapU, con
               int rest, int u0, int ncols, int K, int kpart, int kw, bool bf16, cudaStream_t s, int reserve = 0,
               unsigned* tile_ctr = nullptr, int helper_ctas = 0, const unsigned* amax_in = nullptr) {
   const unsigned* amax = bf16 ? nullptr : (amax_in ? amax_in : h->amax);
+  // the main launch and its helper take the same kernel (one tile numbering)
+  const bool pair = h->gemm_pair && kpart > 0;
   if (helper_ctas > 0)
     return launch_gemm_lowp_persistent(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, K, bf16, amax, h->st,
-                                       h->spin, helper_ctas, s, kpart, tile_ctr);
+                                       h->spin, helper_ctas, s, kpart, tile_ctr, pair);
   const int prods = bf16 ? 1 : (h->cfg.precision == LU_PREC_FP16X3 ? 3 : 1);
   Prof pf(h, s, LU_PH_GEMM, 2.0 * rest * (double)ncols * kw * prods);
   if (h->gemm_ctas > 0)
     return launch_gemm_lowp_persistent(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, K, bf16, amax, h->st,
-                                       h->spin, std::max(1, h->gemm_ctas - reserve), s, kpart, tile_ctr);
+                                       h->spin, std::max(1, h->gemm_ctas - reserve), s, kpart, tile_ctr, pair);
   return launch_gemm_bf16_tc(mapL, mapU, mapC, 0, u0, k1, k1 + u0, rest, ncols, K, bf16, amax, h->st, h->spin, s);
 }
 

@@ -101,6 +101,57 @@ def test_gemm_lowp_persistent_matches_tile_kernel(cuda_dev, M, N, K, mode, pctas
     assert torch.equal(C0, C1)
 
 
+PAIR_BIT = 1 << 24
+
+
+@pytest.mark.parametrize("pctas", [1, 2, 7, 100, 148])
+@pytest.mark.parametrize("M,N,K", [(128, 256, 64), (300, 520, 256), (129, 999, 128), (1000, 700, 192),
+                                   (4096, 4096, 256), (2560, 512, 512)])
+def test_gemm_lowp_cta_pair_kernel(cuda_dev, M, N, K, pctas):
+    """The CTA-pair kernel (tcgen05 cta_group::2, 256 x 256 tiles over two
+    SMs) computes the pairs layout's three products: within the FP32
+    accumulation bound of the exact product of the split operands, the
+    padding columns untouched, and equal to the one-SM pairs kernel."""
+    f = _lib()
+    g = torch.Generator(device="cuda").manual_seed(M * 11 + N + pctas)
+    A = torch.rand(M, K, device="cuda", generator=g, dtype=torch.float32) - 0.5
+    B = (torch.rand(K, N, device="cuda", generator=g, dtype=torch.float32) - 0.5) * 37.0
+    ldc = (N + 3) // 4 * 4 + 4
+    C0 = torch.rand(M, ldc, device="cuda", generator=g, dtype=torch.float32) - 0.5
+    C1 = C0.clone()
+    pad_before = C0[:, N:].clone()
+    ref = _lowp_reference(A, B, C0[:, :N], 3)
+    st = torch.cuda.current_stream().cuda_stream
+    assert f(A.data_ptr(), K, B.data_ptr(), N, C0.data_ptr(), ldc, M, N, K, 3 | (pctas << 8) | PAIR_BIT, st) == 0
+    assert f(A.data_ptr(), K, B.data_ptr(), N, C1.data_ptr(), ldc, M, N, K, 3 | (148 << 8), st) == 0
+    torch.cuda.synchronize()
+    err = (C0[:, :N].double() - ref).abs().max().item()
+    assert err <= 4 * 6e-8 * 3 * K * 0.5 * 18.5 + 1e-6, err
+    assert torch.equal(C0[:, N:], pad_before)
+    assert torch.equal(C0, C1)
+
+
+@pytest.mark.parametrize("pctas,hctas", [(100, 48), (2, 2), (3, 5), (116, 32)])
+@pytest.mark.parametrize("M,N,K", [(300, 520, 256), (1100, 2100, 192), (4096, 4096, 256)])
+def test_gemm_lowp_cta_pair_shared_tile_counter(cuda_dev, M, N, K, pctas, hctas):
+    """Two CTA-pair launches on two streams sharing one tile counter (the
+    even CTA of each pair draws the tile and hands it to the odd one) give
+    the same C as one launch."""
+    f = _lib()
+    g = torch.Generator(device="cuda").manual_seed(M + 9 * N + pctas + hctas)
+    A = torch.rand(M, K, device="cuda", generator=g, dtype=torch.float32) - 0.5
+    B = (torch.rand(K, N, device="cuda", generator=g, dtype=torch.float32) - 0.5) * 5.0
+    ldc = (N + 3) // 4 * 4
+    C0 = torch.rand(M, ldc, device="cuda", generator=g, dtype=torch.float32) - 0.5
+    C1 = C0.clone()
+    st = torch.cuda.current_stream().cuda_stream
+    assert f(A.data_ptr(), K, B.data_ptr(), N, C0.data_ptr(), ldc, M, N, K, 3 | (148 << 8) | PAIR_BIT, st) == 0
+    assert f(A.data_ptr(), K, B.data_ptr(), N, C1.data_ptr(), ldc, M, N, K,
+             3 | (pctas << 8) | (hctas << 16) | PAIR_BIT, st) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(C0, C1)
+
+
 @pytest.mark.parametrize("mode", [0, 2, 3])
 @pytest.mark.parametrize("pctas,hctas", [(100, 48), (1, 1), (3, 5), (116, 32)])
 @pytest.mark.parametrize("M,N,K", [(300, 520, 256), (1100, 2100, 192), (4096, 4096, 256)])
@@ -242,6 +293,33 @@ def test_refine_update_helper_bitwise(cuda_dev, n, b, monkeypatch):
         assert s.status() == 0 and info["status"] == 0, info
         xs.append(x)
     assert torch.equal(xs[0], xs[1])
+
+
+@pytest.mark.parametrize("n,b,la,split", [(4096, 512, True, "0"), (3000, 192, True, "0"), (2048, 512, False, "0"),
+                                         (4096, 512, True, "1")])
+def test_refine_cta_pair_update_bitwise(cuda_dev, n, b, la, split, monkeypatch):
+    """LU_B200_GEMM_PAIR=1 runs the trailing updates (and their helper
+    launches) on CTA pairs; each C element receives the same FP32 increment,
+    so the factors and x are the same bit for bit as with one-SM tiles, also
+    under graph replay."""
+    import charmlu_b200 as lu
+    monkeypatch.setenv("LU_B200_LA_SPLIT", split)
+    A = lu.generate_uniform(n, n, seed=21, stream_id=0)
+    rhs = lu.generate_uniform(n, 1, seed=21, stream_id=1).view(-1)
+    xs = []
+    for pair in ("0", "1"):
+        monkeypatch.setenv("LU_B200_GEMM_PAIR", pair)
+        s = lu.LUSolver(lu.LUConfig(n, b, precision=lu.LU_PREC_FP16X3, lookahead=la))
+        x, info = s.refine_solve(A, rhs)
+        assert s.status() == 0 and info["status"] == 0, info
+        assert s.residual(A, x, rhs)["r_hpl"] < 16
+        xs.append(x)
+    assert torch.equal(xs[0], xs[1])
+    sg = lu.LUSolver(lu.LUConfig(n, b, precision=lu.LU_PREC_FP16X3, lookahead=la, use_graph=True))
+    xg = torch.empty_like(rhs)
+    for _ in range(2):
+        sg.refine_solve(A, rhs, xg)
+        assert sg.status() == 0 and torch.equal(xg, xs[1])
 
 
 @pytest.mark.parametrize("n,b,la", [(4096, 512, True), (3000, 256, True), (2048, 512, False), (1500, 192, True)])
