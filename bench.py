@@ -951,8 +951,11 @@ def main():
         # element for the error-compensated split, one otherwise
         prods = 3 if args.precision == "fp16x3" else 1
         alg_tf = gemm_tf / prods if gemm_tf else None
-        roof = {"bound": "tensor", "kernel": f"gemm_lowp_persistent_kernel (trailing update, tcgen05 kind::f16 "
-                                             f"{args.precision}, double-buffered TMEM accumulators)",
+        # FP16x3 runs on CTA pairs unless LU_B200_GEMM_PAIR=0
+        pair = args.precision == "fp16x3" and os.environ.get("LU_B200_GEMM_PAIR", "1") != "0"
+        kname = ("gemm_lowp_pair_kernel (trailing update, tcgen05 kind::f16 cta_group::2, 256x256 tiles on CTA "
+                 "pairs" if pair else "gemm_lowp_persistent_kernel (trailing update, tcgen05 kind::f16")
+        roof = {"bound": "tensor", "kernel": f"{kname}, {args.precision}, double-buffered TMEM accumulators)",
                 "achieved": alg_tf, "peak": peak_v, "unit": "TFLOP/s",
                 "frac": (alg_tf / peak_v) if alg_tf else None, "traffic": None,
                 "flops_counted": "algorithmic: 2*M*N*K per trailing update, each product once",
@@ -970,7 +973,8 @@ def main():
                     roof["frac_executed_of_sms_held"] = gemm_tf / (peak_v * held / sms)
             except Exception:
                 pass
-        tpath = os.path.join(ROOT, "profiles", "gemm_lowp_persistent_traffic.json")
+        tpath = os.path.join(ROOT, "profiles",
+                             "gemm_lowp_pair_traffic.json" if pair else "gemm_lowp_persistent_traffic.json")
     else:
         roof = {"bound": "tensor", "kernel": "gemm_f64_sub_kernel (trailing update, DMMA)",
                 "achieved": gemm_tf, "peak": peak64_v, "unit": "TFLOP/s",
