@@ -89,10 +89,12 @@ __device__ __forceinline__ void tuning_for(int n, int esize, int& nb, int& small
   // shared-memory caps: small path n x (n+1); blocked path panel m x (nb+1) + nb x 128 staging
   const int small_cap = (int)(sqrtf((float)(kBatchSmem / esize)) - 1.f);
   if (small > small_cap) small = small_cap;
-  // the update phase reuses the same space: U12 slice, two L and two C tiles
+  // the update phase reuses the same space: a U slice and two L tiles of
+  // depth up to the outer block width
+  const size_t ob = esize == 8 ? 64 : 128;
   while (nb > 4) {
     const size_t panel_phase = (size_t)n * (nb + 1) + (size_t)nb * 128;
-    const size_t update_phase = (size_t)nb * 128 + (size_t)2 * 64 * nb + (size_t)2 * 64 * 128;
+    const size_t update_phase = ob * 128 + (size_t)2 * 64 * ob;
     if ((panel_phase > update_phase ? panel_phase : update_phase) * esize <= kBatchSmem) break;
     nb >>= 1;
   }
@@ -103,7 +105,10 @@ __device__ __forceinline__ bool better(T v1, int r1, T v2, int r2) {
   return r1 >= 0 && (r2 < 0 || v1 > v2 || (v1 == v2 && r1 < r2));
 }
 
-// block-wide argmax (value, row); lowest row on ties; -1 if no positive value
+// block-wide argmax (value, row); lowest row on ties; -1 if no positive value.
+// One barrier: every warp reduces the NWARP per-warp candidates itself.  The
+// caller puts a barrier between the return and its next call (the slots are
+// reused).
 template <typename T>
 __device__ int block_argmax(T v, int r, T* sv, int* sr) {
 #pragma unroll
@@ -115,21 +120,15 @@ __device__ int block_argmax(T v, int r, T* sv, int* sr) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (lane == 0) { sv[warp] = v; sr[warp] = r; }
   __syncthreads();
-  if (warp == 0) {
-    v = lane < NWARP ? sv[lane] : T(0);
-    r = lane < NWARP ? sr[lane] : -1;
+  v = lane < NWARP ? sv[lane] : T(0);
+  r = lane < NWARP ? sr[lane] : -1;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      T v2 = __shfl_xor_sync(0xffffffffu, v, o);
-      int r2 = __shfl_xor_sync(0xffffffffu, r, o);
-      if (better(v2, r2, v, r)) { v = v2; r = r2; }
-    }
-    if (lane == 0) sr[NWARP] = r;
+  for (int o = 16; o > 0; o >>= 1) {
+    T v2 = __shfl_xor_sync(0xffffffffu, v, o);
+    int r2 = __shfl_xor_sync(0xffffffffu, r, o);
+    if (better(v2, r2, v, r)) { v = v2; r = r2; }
   }
-  __syncthreads();
-  const int out = sr[NWARP];
-  __syncthreads();
-  return out;
+  return r;
 }
 
 // Unblocked LU with partial pivoting of an m x w block in shared memory
@@ -147,7 +146,9 @@ __device__ int getf2_smem(T* a, int ld, int m, int w, int* piv_s, T* sv, int* sr
     if (v > bv) { bv = v; br = i; }
   }
   for (int j = 0; j < w && j < m; j++) {
-    int p = block_argmax(bv, br, sv, sr);  // its barriers also end the previous update
+    // its barrier also ends the previous update; the barrier after the
+    // swap separates this call from the next
+    int p = block_argmax(bv, br, sv, sr);
     if (p < 0) {
       p = j;
       if (info == 0) info = j + 1;
@@ -245,102 +246,225 @@ __device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async
 template <int N>
 __device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// Trailing update A[c1:n, c1:n] -= L21 * U12 (L21 = A[c1:n, k0:k0+kw], U12 =
-// A[k0:k0+kw, c1:n], both final in global memory) over 64 x 128 tiles, 4 x 4
-// outputs per thread: rows tr*4 .. +3 (one row group per warp: the L reads
-// are broadcasts), columns tc + 32 j (consecutive across lanes: conflict-free
-// shared reads and coalesced global writes).  Per column tile the U12 slice
-// is staged once; the row tiles' C and L blocks stream through two shared
-// buffers with the async copy unit, so the next tile's loads are in flight
-// while this one is computed.  smem (reusing the panel's space):
-//   Ut [nb][128] | Lt[2] [64][nb] | Ct[2] [64][128]
+// Outer block width of the two-level blocking: the inner panels (nb
+// columns) update only the outer block's own columns and U rows; the rest of
+// the trailing matrix gets one update of depth kOuter per outer block.
 template <typename T>
-__device__ void trailing_update(T* A, int n, int k0, int kw, int c1, int nb, unsigned char* smem) {
-  const int tid = threadIdx.x, tr = tid >> 5, tc = tid & 31;
+constexpr int outer_block() { return sizeof(T) == 8 ? 64 : 128; }
+
+// C[r0:r1, c0:c1] -= A[r0:r1, kk0:kk0+K] * A[kk0:kk0+K, c0:c1] (K <=
+// outer_block<T>(); the L and U blocks final in global memory) over TM x TN
+// tiles, a 4 x 4 block of outputs per thread: rows tr*4 .. +3, columns
+// tc + (TN/4) j (consecutive across the lanes of a column group: conflict-free
+// shared reads of U and coalesced global accesses; a warp spans 32*4/TN row
+// groups, whose L rows sit in distinct banks with the pitch K + 1).  Shapes:
+// 64 x 128 for the outer block's trailing update, 256 x 32 for the narrow
+// update of its own columns, 32 x 256 for its U rows.  Per column tile the U
+// slice is staged once; the row tiles' L blocks stream through two shared
+// buffers with the async copy unit.  Each thread's C values are loaded at
+// the start of its tile and subtracted after the products are summed, so
+// their latency hides behind the k loop.
+// smem (reusing the panel's space):  Ut [K][TN] | Lt[2] [TM][K+1]
+template <typename T, int TM, int TN>
+__device__ void update_block(T* A, int n, int r0, int r1, int c0, int c1, int kk0, int K, unsigned char* smem) {
+  static_assert((TM / 4) * (TN / 4) == BT, "one 4 x 4 block of outputs per thread");
+  constexpr int GX = TN / 4;
+  if (r0 >= r1 || c0 >= c1 || K <= 0) return;
+  const int tid = threadIdx.x, tr = tid / GX, tc = tid % GX;
+  const int KP = K + 1;
   T* ut = reinterpret_cast<T*>(smem);
-  T* lt = ut + (size_t)nb * 128;
-  T* ctb = lt + 2 * (size_t)64 * nb;
-  const int nrt = (n - c1 + 63) / 64;
-  auto issue = [&](int t, int ct, int buf) {
-    const int rt = c1 + t * 64;
-    T* cdst = ctb + (size_t)buf * 64 * 128;
-    T* ldst = lt + (size_t)buf * 64 * nb;
-    for (int idx = tid; idx < 64 * 128; idx += BT) {
-      const int r = idx >> 7, c = idx & 127;
-      const bool ok = rt + r < n && ct + c < n;
-      cp_async_elem<sizeof(T)>(cdst + idx, ok ? A + (int64_t)(rt + r) * n + ct + c : A, ok);
-    }
-    for (int idx = tid; idx < 64 * nb; idx += BT) {
-      const int r = idx / nb, p = idx - r * nb;
-      const bool ok = rt + r < n && p < kw;
-      cp_async_elem<sizeof(T)>(ldst + idx, ok ? A + (int64_t)(rt + r) * n + k0 + p : A, ok);
+  T* lt = ut + (size_t)K * TN;
+  const int nrt = (r1 - r0 + TM - 1) / TM;
+  auto issue = [&](int t, int buf) {
+    const int rt = r0 + t * TM;
+    T* ldst = lt + (size_t)buf * TM * KP;
+    for (int idx = tid; idx < TM * K; idx += BT) {
+      const int r = idx / K, p = idx - r * K;
+      const bool ok = rt + r < r1;
+      cp_async_elem<sizeof(T)>(ldst + r * KP + p, ok ? A + (int64_t)(rt + r) * n + kk0 + p : A, ok);
     }
     cp_async_commit_group();
   };
-  for (int ct = c1; ct < n; ct += 128) {
-    // U12 slice (kw x 128): all of a thread's loads in flight together
-    for (int base = 0; base < kw * 128; base += BT * 8) {
+  for (int ct = c0; ct < c1; ct += TN) {
+    // U slice (K x TN): all of a thread's loads in flight together
+    for (int base = 0; base < K * TN; base += BT * 8) {
       T v[8];
 #pragma unroll
       for (int u = 0; u < 8; u++) {
         const int idx = base + tid + u * BT;
-        const int p = idx >> 7, c = idx & 127;
-        v[u] = (idx < kw * 128 && ct + c < n) ? A[(int64_t)(k0 + p) * n + ct + c] : T(0);
+        const int p = idx / TN, c = idx % TN;
+        v[u] = (idx < K * TN && ct + c < c1) ? A[(int64_t)(kk0 + p) * n + ct + c] : T(0);
       }
 #pragma unroll
       for (int u = 0; u < 8; u++) {
         const int idx = base + tid + u * BT;
-        if (idx < kw * 128) ut[idx] = v[u];
+        if (idx < K * TN) ut[idx] = v[u];
       }
     }
-    issue(0, ct, 0);
+    issue(0, 0);
     for (int t = 0; t < nrt; t++) {
       const int buf = t & 1;
+      const int rbase = r0 + t * TM + tr * 4;
+      T cv[4][4];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int r = rbase + i, c = ct + tc + GX * j;
+          cv[i][j] = (r < r1 && c < c1) ? A[(int64_t)r * n + c] : T(0);
+        }
       if (t + 1 < nrt) {
-        issue(t + 1, ct, buf ^ 1);
+        issue(t + 1, buf ^ 1);
         cp_async_wait_group<1>();
       } else {
         cp_async_wait_group<0>();
       }
-      __syncthreads();  // tile t (and, at t = 0, the U12 slice) in shared memory
-      const T* cs = ctb + (size_t)buf * 64 * 128;
-      const T* ls = lt + (size_t)buf * 64 * nb;
+      __syncthreads();  // L tile t (and, at t = 0, the U slice) in shared memory
+      const T* ls = lt + (size_t)buf * TM * KP + (size_t)tr * 4 * KP;
       T acc[4][4];
 #pragma unroll
       for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = cs[(tr * 4 + i) * 128 + tc + 32 * j];
-      for (int p = 0; p < kw; p++) {
+        for (int j = 0; j < 4; j++) acc[i][j] = T(0);
+      for (int p = 0; p < K; p++) {
         T av[4], bv[4];
 #pragma unroll
-        for (int i = 0; i < 4; i++) av[i] = ls[(tr * 4 + i) * nb + p];
+        for (int i = 0; i < 4; i++) av[i] = ls[i * KP + p];
 #pragma unroll
-        for (int j = 0; j < 4; j++) bv[j] = ut[p * 128 + tc + 32 * j];
+        for (int j = 0; j < 4; j++) bv[j] = ut[p * TN + tc + GX * j];
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
-          for (int j = 0; j < 4; j++) acc[i][j] = fma(-av[i], bv[j], acc[i][j]);
+          for (int j = 0; j < 4; j++) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
       }
-      const int rbase = c1 + t * 64 + tr * 4;
 #pragma unroll
       for (int i = 0; i < 4; i++) {
         const int r = rbase + i;
-        if (r >= n) break;
+        if (r >= r1) break;
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-          const int c = ct + tc + 32 * j;
-          if (c < n) A[(int64_t)r * n + c] = acc[i][j];
+          const int c = ct + tc + GX * j;
+          if (c < c1) A[(int64_t)r * n + c] = cv[i][j] - acc[i][j];
         }
       }
-      __syncthreads();  // buffer `buf` (and the U12 slice after the last tile) free for reuse
+      __syncthreads();  // buffer `buf` (and the U slice after the last tile) free for reuse
     }
   }
 }
 
-// Factor A (n x n row-major in global, ld = n) in place, permuting x along
-// with the rows and recording the pivots (global rows) in piv.
+// First q < np with key[q] == v, found by one warp (all lanes get it); -1 if none.
+__device__ __forceinline__ int warp_find(const int* key, int np, int v) {
+  const int lane = threadIdx.x & 31;
+  for (int base = 0; base < np; base += 32) {
+    const unsigned m = __ballot_sync(0xffffffffu, base + lane < np && key[base + lane] == v);
+    if (m) return base + __ffs(m) - 1;
+  }
+  return -1;
+}
+
+// One warp: the interchanges (K0 + j) <-> piv[K0 + j], j = 0 .. S-1, in order,
+// composed into one simultaneous assignment row mdst[q] <- row msrc[q]
+// (q < the returned count, at most 2 S rows); pos / cont are scratch of 2 S.
+__device__ int compose_moves(const int* piv, int K0, int S, int* pos, int* cont, int* mdst, int* msrc) {
+  const int lane = threadIdx.x & 31;
+  int np = 0;
+  for (int j = 0; j < S; j++) {
+    const int a = K0 + j, b = piv[K0 + j];
+    if (a == b) continue;
+    int ia = warp_find(pos, np, a);
+    if (ia < 0) {
+      if (lane == 0) { pos[np] = a; cont[np] = a; }
+      ia = np++;
+      __syncwarp();
+    }
+    int ib = warp_find(pos, np, b);
+    if (ib < 0) {
+      if (lane == 0) { pos[np] = b; cont[np] = b; }
+      ib = np++;
+      __syncwarp();
+    }
+    if (lane == 0) {
+      const int t = cont[ia];
+      cont[ia] = cont[ib];
+      cont[ib] = t;
+    }
+    __syncwarp();
+  }
+  int mm = 0;
+  for (int base = 0; base < np; base += 32) {
+    const int q = base + lane;
+    const bool mv = q < np && pos[q] != cont[q];
+    const unsigned m = __ballot_sync(0xffffffffu, mv);
+    if (mv) {
+      const int o = mm + __popc(m & ((1u << lane) - 1u));
+      mdst[o] = pos[q];
+      msrc[o] = cont[q];
+    }
+    mm += __popc(m);
+  }
+  __syncwarp();
+  return mm;
+}
+
+// Row moves A[mdst[q], ca:cb] <- A[msrc[q], ca:cb] (q < mm <= 256), every
+// source read before any destination is written: 128-column chunks staged in
+// shared memory (buf, mm x 128 elements), 16 loads in flight per thread.
 template <typename T>
-__device__ int factor_system(T* A, int n, T* x, int* piv, unsigned char* smem, T* sv, int* sr, int* piv_s) {
+__device__ void apply_moves(T* A, int n, const int* mdst, const int* msrc, int mm, int ca, int cb, T* buf) {
+  const int tid = threadIdx.x;
+  const int tot = mm * 128;
+  for (int c0 = ca; c0 < cb; c0 += 128) {
+    const int w = min(128, cb - c0);
+    for (int base = 0; base < tot; base += BT * 16) {
+      T v[16];
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const int idx = base + tid + u * BT;
+        const int q = idx >> 7, c = idx & 127;
+        v[u] = (idx < tot && c < w) ? A[(int64_t)msrc[q] * n + c0 + c] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const int idx = base + tid + u * BT;
+        if (idx < tot) buf[idx] = v[u];
+      }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < tot; idx += BT) {
+      const int q = idx >> 7, c = idx & 127;
+      if (c < w) A[(int64_t)mdst[q] * n + c0 + c] = buf[idx];
+    }
+    __syncthreads();
+  }
+}
+
+// U rows: A[k0:k0+kw, c0:c1] <- L^{-1} A[k0:k0+kw, c0:c1], L the kw x kw
+// unit-lower block at lsm (pitch ld, shared memory); one column per thread.
+template <typename T>
+__device__ void u_rows(T* A, int n, int k0, int kw, int c0, int c1, const T* lsm, int ld) {
+  for (int c = c0 + threadIdx.x; c < c1; c += BT) {
+    T u[32];
+#pragma unroll
+    for (int i = 0; i < 32; i++) u[i] = i < kw ? A[(int64_t)(k0 + i) * n + c] : T(0);
+#pragma unroll
+    for (int i = 1; i < 32; i++) {
+      if (i >= kw) break;
+#pragma unroll
+      for (int p = 0; p < 32; p++) {
+        if (p >= i) break;
+        u[i] = fma(-lsm[i * ld + p], u[p], u[i]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 32; i++)
+      if (i < kw) A[(int64_t)(k0 + i) * n + c] = u[i];
+  }
+}
+
+// Factor A (n x n row-major in global, ld = n) in place, recording the
+// pivots (global rows, LAPACK order) in piv; the caller permutes b.
+template <typename T>
+__device__ int factor_system(T* A, int n, int* piv, unsigned char* smem, T* sv, int* sr, int* piv_s) {
   const int tid = threadIdx.x;
   int nb, small;
   tuning_for(n, (int)sizeof(T), nb, small);
@@ -350,14 +474,7 @@ __device__ int factor_system(T* A, int n, T* x, int* piv, unsigned char* smem, T
     for (int idx = tid; idx < n * n; idx += BT) a[(idx / n) * ld + idx % n] = A[idx];
     __syncthreads();
     const int info = getf2_smem(a, ld, n, n, piv_s, sv, sr);
-    // pivots -> x and global record (sequential swaps by one thread)
-    if (tid == 0) {
-      for (int j = 0; j < n; j++) {
-        const int p = piv_s[j];
-        piv[j] = p;
-        if (p != j) { const T t = x[j]; x[j] = x[p]; x[p] = t; }
-      }
-    }
+    for (int j = tid; j < n; j += BT) piv[j] = piv_s[j];
     for (int idx = tid; idx < n * n; idx += BT) A[idx] = a[(idx / n) * ld + idx % n];
     __syncthreads();
     return info;
@@ -366,6 +483,8 @@ __device__ int factor_system(T* A, int n, T* x, int* piv, unsigned char* smem, T
   const int ld = nb + 1;
   T* panel = reinterpret_cast<T*>(smem);                  // n x (nb+1)
   __shared__ int sw_dst[64], sw_src[64], sw_m;             // composed row moves of a panel
+  // an outer block's composed interchanges (at most 2 x outer_block rows)
+  __shared__ int s_pos[256], s_cont[256], s_mdst[256], s_msrc[256];
   for (int k0 = 0; k0 < n; k0 += nb) {
     const int kw = min(nb, n - k0), m = n - k0;
     // panel in: eight loads in flight per thread
@@ -391,84 +510,110 @@ __device__ int factor_system(T* A, int n, T* x, int* piv, unsigned char* smem, T
       const int i = idx / kw, c = idx - i * kw;
       A[(int64_t)(k0 + i) * n + k0 + c] = panel[i * ld + c];
     }
-    // the panel's swaps, in order, composed into one assignment of the
-    // affected rows (row dst <- row src, at most 2 kw moves), then applied to
-    // the columns outside the panel with every source read before any
-    // destination is written; x and the pivot record by thread 0 in order
-    if (tid == 0) {
-      int pos[64], cont[64], np = 0;
-      for (int j = 0; j < kw; j++) {
-        const int p = piv_s[j];
-        piv[k0 + j] = k0 + p;
-        if (p != j) {
-          const T t = x[k0 + j];
-          x[k0 + j] = x[k0 + p];
-          x[k0 + p] = t;
-          int ia = -1, ib = -1;
-          for (int q = 0; q < np; q++) {
-            if (pos[q] == j) ia = q;
-            if (pos[q] == p) ib = q;
-          }
-          if (ia < 0) { pos[np] = j; cont[np] = j; ia = np++; }
-          if (ib < 0) { pos[np] = p; cont[np] = p; ib = np++; }
-          const int t2 = cont[ia];
-          cont[ia] = cont[ib];
-          cont[ib] = t2;
-        }
-      }
-      int mm = 0;
-      for (int q = 0; q < np; q++)
-        if (pos[q] != cont[q]) { sw_dst[mm] = k0 + pos[q]; sw_src[mm] = k0 + cont[q]; mm++; }
-      sw_m = mm;
+    // Two-level blocking.  Inside an outer block of NB columns each panel
+    // swaps rows, solves its U rows and updates all rows below only within
+    // the outer block's columns.  The columns left and right of the outer
+    // block are untouched until its last panel: then its interchanges,
+    // composed into one assignment of rows, are applied to them in one pass;
+    // its U rows right of it are solved (blocked forward substitution with its
+    // unit-lower L11); and the rest of the trailing matrix gets one update of
+    // depth NB.
+    constexpr int NB = outer_block<T>();
+    const int K0 = k0 - k0 % NB, Kend = min(n, K0 + NB);
+    const int c1 = k0 + kw;
+    // this panel's swaps (the pivot record, then one warp composes them into
+    // one assignment of the affected rows: row dst <- row src, at most 2 kw
+    // moves), applied to the outer block's other columns with every source
+    // read before any destination is written
+    for (int j = tid; j < kw; j += BT) piv[k0 + j] = k0 + piv_s[j];
+    __syncthreads();
+    if (tid < 32) {
+      const int mm = compose_moves(piv, k0, kw, s_pos, s_cont, sw_dst, sw_src);
+      if (tid == 0) sw_m = mm;
     }
     __syncthreads();
     {
-      const int mm = sw_m;
-      // four threads per column, each a quarter of the moves (<= 16)
-      const int q4 = tid & 3;
-      for (int cb = 0; cb < n - kw; cb += BT / 4) {
-        const int c = cb + (tid >> 2);
-        const int col = c < k0 ? c : c + kw;
-        const bool live = c < n - kw;
-        T v[16];
+      // at most NB - kw <= 120 columns: four threads per column, each a
+      // quarter of the moves (<= 16)
+      const int mm = sw_m, nleft = k0 - K0, ncols = nleft + (Kend - c1);
+      const int q4 = tid & 3, c = tid >> 2;
+      const bool live = c < ncols;
+      const int col = c < nleft ? K0 + c : c1 + (c - nleft);
+      T v[16];
 #pragma unroll
-        for (int u = 0; u < 16; u++) {
-          const int q = q4 + 4 * u;
-          v[u] = (live && q < mm) ? A[(int64_t)sw_src[q] * n + col] : T(0);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int u = 0; u < 16; u++) {
-          const int q = q4 + 4 * u;
-          if (live && q < mm) A[(int64_t)sw_dst[q] * n + col] = v[u];
-        }
-        __syncthreads();
+      for (int u = 0; u < 16; u++) {
+        const int q = q4 + 4 * u;
+        v[u] = (live && q < mm) ? A[(int64_t)sw_src[q] * n + col] : T(0);
       }
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const int q = q4 + 4 * u;
+        if (live && q < mm) A[(int64_t)sw_dst[q] * n + col] = v[u];
+      }
+      __syncthreads();
     }
-    const int c1 = k0 + kw, nr = n - c1;
-    if (nr <= 0) break;
-    // U row: A[k0:k0+kw, c1:n] <- L11^{-1} A[k0:k0+kw, c1:n]  (one column per thread)
-    for (int c = c1 + tid; c < n; c += BT) {
-      T u[32];
-#pragma unroll
-      for (int i = 0; i < 32; i++) u[i] = i < kw ? A[(int64_t)(k0 + i) * n + c] : T(0);
-#pragma unroll
-      for (int i = 1; i < 32; i++) {
-        if (i >= kw) break;
-#pragma unroll
-        for (int p = 0; p < 32; p++) {
-          if (p >= i) break;
-          u[i] = fma(-panel[i * ld + p], u[p], u[i]);
-        }
-      }
-#pragma unroll
-      for (int i = 0; i < 32; i++)
-        if (i < kw) A[(int64_t)(k0 + i) * n + c] = u[i];
+    if (c1 < Kend) {
+      u_rows<T>(A, n, k0, kw, c1, Kend, panel, ld);
+      __syncthreads();
+      update_block<T, 256, 32>(A, n, c1, n, c1, Kend, k0, kw, smem);
+      continue;
+    }
+    // the outer block's last panel: its interchanges on the other columns
+    if (tid < 32) {
+      const int mm = compose_moves(piv, K0, Kend - K0, s_pos, s_cont, s_mdst, s_msrc);
+      if (tid == 0) sw_m = mm;
     }
     __syncthreads();
-    trailing_update<T>(A, n, k0, kw, c1, nb, smem);
+    apply_moves<T>(A, n, s_mdst, s_msrc, sw_m, 0, K0, reinterpret_cast<T*>(smem));
+    apply_moves<T>(A, n, s_mdst, s_msrc, sw_m, Kend, n, reinterpret_cast<T*>(smem));
+    if (Kend >= n) break;
+    T* dg = reinterpret_cast<T*>(smem);  // [32][33]: one diagonal block of L11
+    for (int q0 = K0; q0 < Kend; q0 += nb) {
+      const int qw = min(nb, Kend - q0);
+      for (int idx = tid; idx < qw * qw; idx += BT) {
+        const int i = idx / qw, p = idx - i * qw;
+        dg[i * 33 + p] = A[(int64_t)(q0 + i) * n + q0 + p];
+      }
+      __syncthreads();
+      u_rows<T>(A, n, q0, qw, Kend, n, dg, 33);
+      __syncthreads();
+      update_block<T, 32, 256>(A, n, q0 + qw, Kend, Kend, n, q0, qw, smem);
+    }
+    update_block<T, 64, 128>(A, n, Kend, n, Kend, n, K0, Kend - K0, smem);
   }
   return info;
+}
+
+// perm[i] = the original row that the interchanges j <-> piv[j] (j = 0 ..
+// n-1, in order) bring to row i; piv is copied to shared memory (scratch, n
+// ints) and one thread composes the sequence there.
+__device__ void pivots_to_perm(const int* piv, int n, int* perm, int* scratch) {
+  const int tid = threadIdx.x;
+  for (int i = tid; i < n; i += BT) {
+    perm[i] = i;
+    scratch[i] = piv[i];
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int j = 0; j < n; j++) {
+      const int p = scratch[j];
+      if (p != j) {
+        const int t = perm[j];
+        perm[j] = perm[p];
+        perm[p] = t;
+      }
+    }
+  __syncthreads();
+}
+
+// x <- P x, x[i] <- x[perm[i]], through shared memory (buf: n elements)
+template <typename T>
+__device__ void gather_perm(T* x, int n, const int* perm, T* buf) {
+  for (int i = threadIdx.x; i < n; i += BT) buf[i] = x[perm[i]];
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += BT) x[i] = buf[i];
+  __syncthreads();
 }
 
 __global__ void __launch_bounds__(BT, 1) batched_kernel(BatchArgs a) {
@@ -482,9 +627,9 @@ __global__ void __launch_bounds__(BT, 1) batched_kernel(BatchArgs a) {
   float* A32s = reinterpret_cast<float*>(a.work + hdr->A32);
   double* r64s = reinterpret_cast<double*>(a.work + hdr->r64);
   float* v32s = reinterpret_cast<float*>(a.work + hdr->v32);
-  __shared__ double sv_d[NWARP + 1];
-  __shared__ float sv_f[NWARP + 1];
-  __shared__ int sr[NWARP + 1];
+  __shared__ double sv_d[NWARP];
+  __shared__ float sv_f[NWARP];
+  __shared__ int sr[NWARP];
   __shared__ int piv_s[kBatchMaxN];
   __shared__ double s_acc_d[32];
   __shared__ float s_acc_f[32];
@@ -504,8 +649,10 @@ __global__ void __launch_bounds__(BT, 1) batched_kernel(BatchArgs a) {
     int* piv = pivs + offV[sys];
     int info = 0;
     if (a.precision == LU_PREC_FP64) {
-      info = factor_system<double>(A, n, b, piv, smem, sv_d, sr, piv_s);
+      info = factor_system<double>(A, n, piv, smem, sv_d, sr, piv_s);
       __syncthreads();
+      pivots_to_perm(piv, n, piv_s, reinterpret_cast<int*>(smem));
+      gather_perm<double>(b, n, piv_s, reinterpret_cast<double*>(smem));
       solve_global<double>(A, n, b, s_acc_d);
     } else {
       float* A32 = A32s + offA32[sys];
@@ -517,8 +664,11 @@ __global__ void __launch_bounds__(BT, 1) batched_kernel(BatchArgs a) {
         v[i] = (float)b[i];
       }
       __syncthreads();
-      info = factor_system<float>(A32, n, v, piv, smem, sv_f, sr, piv_s);
+      info = factor_system<float>(A32, n, piv, smem, sv_f, sr, piv_s);
       __syncthreads();
+      // piv_s keeps the permutation for the refinement steps
+      pivots_to_perm(piv, n, piv_s, reinterpret_cast<int*>(smem));
+      gather_perm<float>(v, n, piv_s, reinterpret_cast<float*>(smem));
       solve_global<float>(A32, n, v, s_acc_f);
       // x = v, then FP64 refinement: r = b - A x (against the FP64 A), stop
       // when the scaled residual r_hpl < 16, else v = P r, FP32 solve, x += v
@@ -586,14 +736,7 @@ __global__ void __launch_bounds__(BT, 1) batched_kernel(BatchArgs a) {
           if (tid == 0) atomicAdd(&hdr->refine_hist[kRefineHistBins - 1], 1);
           break;
         }
-        if (tid == 0) {
-          for (int j = 0; j < n; j++) {
-            const int p = piv[j];
-            if (p != j) { const double t = r[j]; r[j] = r[p]; r[p] = t; }
-          }
-        }
-        __syncthreads();
-        for (int i = tid; i < n; i += BT) v[i] = (float)r[i];
+        for (int i = tid; i < n; i += BT) v[i] = (float)r[piv_s[i]];
         __syncthreads();
         solve_global<float>(A32, n, v, s_acc_f);
         for (int i = tid; i < n; i += BT) b[i] += (double)v[i];
