@@ -72,6 +72,7 @@ struct lu_handle_s {
   // mixed path: the panels' inner TRSMs (w <= 256) as one blocked launch
   // instead of the recursion (LU_B200_TRSM_BLOCK=0 restores the recursion)
   int trsm_block = 1;
+  int trsm_wide = 1;  // mixed U block-row solves (w <= 512, > 512 columns) in one launch with inverted diagonal blocks
   lub::TsluScratch tslu_scr{};
   // FP16x3 mixed path: the recursive FP32 panel's GEMM halves of width >= 128
   // on the tcgen05 kernel, with their own split-operand buffers (the panel
@@ -94,6 +95,7 @@ struct lu_handle_s {
   lub::ResidualAccum* racc_host = nullptr;
   // mixed-precision workspace (allocated on first use)
   float* A32 = nullptr;        // FP32 working copy, n x ld32
+  float* dinv32 = nullptr;     // inverses of the 32 x 32 diagonal blocks of a panel's L11 (wide U solve)
   int64_t ld32 = 0;
   __nv_bfloat16* Lb = nullptr; // BF16 L21 panel, n x ldk (K-major)
   __nv_bfloat16* Ub = nullptr; // BF16 U12^T panel, n x ldk (K-major)

@@ -94,6 +94,9 @@ template <typename T>
 int launch_trsm_llu_leaf(const T* L, int64_t ldl, T* B, int64_t ldb, int m, int ncols, cudaStream_t s);
 // FP32 B(w x ncols) <- L^{-1} B, L unit lower w x w, w <= 256, one launch
 int launch_trsm_llu_block(const float* L, int64_t ldl, float* B, int64_t ldb, int w, int ncols, cudaStream_t s);
+// B (w x ncols) <- L^{-1} B, L unit lower, w <= 512, FP32; dinv: 16 x 1024 floats of scratch
+int launch_trsm_wide(const float* L, int64_t ldl, float* B, int64_t ldb, int w, int ncols, float* dinv,
+                     cudaStream_t s);
 // single/multi right-hand side substitution with flags (persistent tickets)
 template <typename T>
 int launch_trsv(const T* LU, int64_t lda, int n, T* x, int upper, int* flags, unsigned* ticket, DevStatus* st,

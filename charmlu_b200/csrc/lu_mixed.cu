@@ -44,6 +44,7 @@ int ensure_mixed(lu_handle h) {
   LUB_TRY(h->alloc(&h->Ub, (size_t)n * h->ldk));
   LUB_TRY(h->alloc(&h->ipiv32, n));
   LUB_TRY(h->alloc(&h->amax, 4));
+  LUB_TRY(h->alloc(&h->dinv32, 16 * 1024));
   if (h->pairs && h->panel_tc) {  // panel GEMM operands: K <= B/2 rows of [hi | lo], N <= B/2 columns
     h->ldkP = 2 * ((B / 2 + 63) & ~int64_t(63));
     LUB_TRY(h->alloc(&h->Lp, (size_t)n * h->ldkP));
@@ -122,10 +123,18 @@ int sgemm(Ctx32& c, int rc, int cc, int ra, int ca, int rb, int cb, int M, int N
 }
 
 int trsm32(Ctx32& c, int r0, int w, int rb, int cb, int ncols) {
-  if (w > 32 && w <= 256 && ncols <= 512 && c.h->trsm_block) {  // the panels' inner solves: one launch
+  // the panels' inner solves (and, with trsm_block 2, every solve of w <= 256): one launch
+  if (w > 32 && w <= 256 && (ncols <= 512 || c.h->trsm_block == 2) && c.h->trsm_block) {
     Prof pf(c.h, c.s, LU_PH_TRSM, (double)w * w * ncols);
     return launch_trsm_llu_block(c.A + (int64_t)r0 * c.ld + r0, c.ld, c.A + (int64_t)rb * c.ld + cb, c.ld, w, ncols,
                                  c.s);
+  }
+  // a step's U block row (every trailing column): one launch, 32 x 32
+  // diagonal blocks inverted first
+  if (w > 32 && w <= 512 && ncols > 512 && c.h->trsm_wide) {
+    Prof pf(c.h, c.s, LU_PH_TRSM, (double)w * w * ncols);
+    return launch_trsm_wide(c.A + (int64_t)r0 * c.ld + r0, c.ld, c.A + (int64_t)rb * c.ld + cb, c.ld, w, ncols,
+                            c.h->dinv32, c.s);
   }
   if (w <= 32) {
     Prof pf(c.h, c.s, LU_PH_TRSM, (double)w * w * ncols);

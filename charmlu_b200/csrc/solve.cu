@@ -118,6 +118,213 @@ __global__ void __launch_bounds__(kTrsmNT) trsm_llu_block_kernel(const float* __
   }
 }
 
+// ---------------------------------------------------------------------------
+// B (w x ncols) <- L^{-1} B for a wide right-hand block (the U block row of a
+// mixed-path step: w = the panel width <= 512, ncols = every trailing
+// column), FP32.  The inverses of L's 32 x 32 unit-lower diagonal blocks
+// are formed first (tri_inv32_kernel, one CTA each), so every step of the
+// block forward substitution is a product:
+//   x_k = Dinv_k B_k,   B_below -= L_below,k x_k      (k = 0 .. w/32 - 1)
+// Each CTA keeps a 32-column slice of B in shared memory for the whole
+// solve and streams the L block columns through two shared buffers with
+// the async copy unit (block k+1 in flight while block k is applied).
+// Threads: 8 column groups of 4 x 64 rows; each thread updates 4 x 4 blocks
+// (rows ty + 64 j, columns 4 tx ..): the x rows are read as float4
+// broadcasts, the L rows at pitch 36 land in distinct banks.  This replaces
+// the recursion's 16 leaf solves and 15 skinny GEMMs per step, which ran
+// alone on the GPU between two panels.
+// ---------------------------------------------------------------------------
+constexpr int kWideMaxW = 512;
+constexpr int kWideCB = 32;   // columns of B per CTA
+constexpr int kWideNT = 256;
+constexpr int kWideBP = 36;   // pitch of the B slice (16-byte rows, 8 rows in distinct banks)
+constexpr int kWideLP = 36;   // pitch of a staged L block column (16-byte rows, 8 rows in distinct banks)
+constexpr int kWideLBUF = (kWideMaxW - 32) * kWideLP;
+constexpr size_t kWideSmem =
+    ((size_t)kWideMaxW * kWideBP + 2 * (size_t)kWideLBUF + 2 * 1024) * sizeof(float);
+
+// dinv[b] (32 x 32, row-major) = inverse of the unit-lower diagonal block b
+// of L (w x w), rows / columns past w treated as identity
+__global__ void __launch_bounds__(32) tri_inv32_kernel(const float* __restrict__ L, int64_t ldl, int w,
+                                                       float* __restrict__ dinv) {
+  __shared__ float sL[32][33];
+  const int b = blockIdx.x, j = threadIdx.x, k0 = 32 * b, kb = min(32, w - k0);
+#pragma unroll 4
+  for (int i = 0; i < 32; i++) sL[i][j] = (i < kb && j < i) ? L[(int64_t)(k0 + i) * ldl + k0 + j] : 0.f;
+  __syncthreads();
+  // column j of the inverse: forward substitution on e_j
+  float x[32];
+#pragma unroll
+  for (int i = 0; i < 32; i++) x[i] = i == j ? 1.f : 0.f;
+#pragma unroll
+  for (int i = 1; i < 32; i++) {
+#pragma unroll
+    for (int p = 0; p < i; p++) x[i] = fmaf(-sL[i][p], x[p], x[i]);
+  }
+  float* d = dinv + (size_t)b * 1024;
+#pragma unroll
+  for (int i = 0; i < 32; i++) d[i * 32 + j] = x[i];
+}
+
+__device__ __forceinline__ void cp_async16_zfill(void* sdst, const void* gsrc, bool pred) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(sdst)), "l"(gsrc), "r"(pred ? 16 : 0)
+               : "memory");
+}
+
+
+// B rows r0 + ty + 64 i (i < NI, those below r0 + Rp) -= L_k rows x x_k,
+// columns 8 tx .. 8 tx + 7.  Per 4 k: four x row segments (the same for the
+// whole warp: broadcasts) and one float4 of L per row (8 consecutive rows of
+// a quarter-warp in distinct banks) feed 32 NI FMAs per thread.  Rows past
+// Rp read row Rp - 1 and are not stored.
+template <int NI>
+__device__ __forceinline__ void wide_update8(float* sB, const float* Ls, int r0, int Rp, int k0, int tx, int ty) {
+  float c[NI][8];
+  int lo[NI];
+#pragma unroll
+  for (int i = 0; i < NI; i++) {
+    const int rr = ty + 64 * i;
+    lo[i] = min(rr, Rp - 1) * kWideLP;
+    if (rr < Rp) {
+      const float4 a = *reinterpret_cast<const float4*>(&sB[(r0 + rr) * kWideBP + tx * 8]);
+      const float4 b = *reinterpret_cast<const float4*>(&sB[(r0 + rr) * kWideBP + tx * 8 + 4]);
+      c[i][0] = a.x; c[i][1] = a.y; c[i][2] = a.z; c[i][3] = a.w;
+      c[i][4] = b.x; c[i][5] = b.y; c[i][6] = b.z; c[i][7] = b.w;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 8; q++) c[i][q] = 0.f;
+    }
+  }
+#pragma unroll 2
+  for (int k = 0; k < 32; k += 4) {
+    float xv[4][8];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const float4 a = *reinterpret_cast<const float4*>(&sB[(k0 + k + q) * kWideBP + tx * 8]);
+      const float4 b = *reinterpret_cast<const float4*>(&sB[(k0 + k + q) * kWideBP + tx * 8 + 4]);
+      xv[q][0] = a.x; xv[q][1] = a.y; xv[q][2] = a.z; xv[q][3] = a.w;
+      xv[q][4] = b.x; xv[q][5] = b.y; xv[q][6] = b.z; xv[q][7] = b.w;
+    }
+#pragma unroll
+    for (int i = 0; i < NI; i++) {
+      const float4 l = *reinterpret_cast<const float4*>(&Ls[lo[i] + k]);
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        float v = c[i][e];
+        v = fmaf(-l.x, xv[0][e], v);
+        v = fmaf(-l.y, xv[1][e], v);
+        v = fmaf(-l.z, xv[2][e], v);
+        v = fmaf(-l.w, xv[3][e], v);
+        c[i][e] = v;
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NI; i++) {
+    const int rr = ty + 64 * i;
+    if (rr < Rp) {
+      *reinterpret_cast<float4*>(&sB[(r0 + rr) * kWideBP + tx * 8]) = make_float4(c[i][0], c[i][1], c[i][2], c[i][3]);
+      *reinterpret_cast<float4*>(&sB[(r0 + rr) * kWideBP + tx * 8 + 4]) =
+          make_float4(c[i][4], c[i][5], c[i][6], c[i][7]);
+    }
+  }
+}
+
+// VEC: L, B, ldl and ldb allow 16-byte copies (else element loads)
+template <bool VEC>
+__global__ void __launch_bounds__(kWideNT, 1) trsm_wide_kernel(const float* __restrict__ L, int64_t ldl,
+                                                              const float* __restrict__ dinv, float* __restrict__ B,
+                                                              int64_t ldb, int w, int ncols) {
+  extern __shared__ __align__(16) float wide_smem[];
+  float* sB = wide_smem;                                  // [32 nkb][kWideBP]
+  float* sL = wide_smem + (size_t)kWideMaxW * kWideBP;    // [2][w - 32][kWideLP]
+  float* sD = sL + 2 * kWideLBUF;                         // [2][32][32]: Dinv of blocks k, k + 1
+  const int tid = threadIdx.x;
+  const int c0 = blockIdx.x * kWideCB, nc = min(kWideCB, ncols - c0);
+  const int nkb = (w + 31) / 32, wp = nkb * 32;
+  if (VEC && nc == kWideCB) {
+    for (int idx = tid; idx < wp * 8; idx += kWideNT) {
+      const int r = idx >> 3, q = idx & 7;
+      cp_async16_zfill(&sB[r * kWideBP + q * 4], B + (int64_t)min(r, w - 1) * ldb + c0 + q * 4, r < w);
+    }
+  } else {
+    for (int idx = tid; idx < wp * 32; idx += kWideNT) {
+      const int r = idx >> 5, c = idx & 31;
+      sB[r * kWideBP + c] = (r < w && c < nc) ? B[(int64_t)r * ldb + c0 + c] : 0.f;
+    }
+  }
+  // Dinv_k, and the L block column k: rows 32 (k + 1) .. w, columns
+  // 32 k .. 32 k + 31 (all inside L, since a block with rows below it is a
+  // whole 32 columns), zero rows up to the padded height wp
+  auto stage = [&](int k) {
+    const int k0 = 32 * k, r0 = k0 + 32, R = w - r0, Rp = wp - r0;
+    float* dd = sD + (k & 1) * 1024;
+    cp_async16_zfill(&dd[tid * 4], dinv + (size_t)k * 1024 + tid * 4, true);
+    float* dst = sL + (size_t)(k & 1) * kWideLBUF;
+    if (VEC) {
+      for (int idx = tid; idx < Rp * 8; idx += kWideNT) {
+        const int r = idx >> 3, q = idx & 7;
+        cp_async16_zfill(&dst[r * kWideLP + q * 4], L + (int64_t)(r0 + min(r, R - 1)) * ldl + k0 + q * 4, r < R);
+      }
+    } else {
+      for (int idx = tid; idx < Rp * 32; idx += kWideNT) {
+        const int r = idx >> 5, c = idx & 31;
+        dst[r * kWideLP + c] = r < R ? L[(int64_t)(r0 + r) * ldl + k0 + c] : 0.f;
+      }
+    }
+  };
+  stage(0);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  const int tx = tid >> 6, ty = tid & 63;   // update: 8 columns from 8 tx, rows ty + 64 i
+  const int xr = tid >> 3, xc = tid & 7;    // x: row xr, columns 4 xc ..
+  for (int k = 0; k < nkb; k++) {
+    const int k0 = 32 * k, r0 = k0 + 32, Rp = wp - r0;
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();  // B slice, Dinv_k and L block k in shared memory; step k-1 done with the other buffers
+    if (k + 1 < nkb) stage(k + 1);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    // x_k = Dinv_k B_k
+    {
+      const float* drow = sD + (k & 1) * 1024 + xr * 32;
+      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int p = 0; p < 32; p += 4) {
+        const float4 d = *reinterpret_cast<const float4*>(drow + p);
+        const float4 b0 = *reinterpret_cast<const float4*>(&sB[(k0 + p) * kWideBP + xc * 4]);
+        const float4 b1 = *reinterpret_cast<const float4*>(&sB[(k0 + p + 1) * kWideBP + xc * 4]);
+        const float4 b2 = *reinterpret_cast<const float4*>(&sB[(k0 + p + 2) * kWideBP + xc * 4]);
+        const float4 b3 = *reinterpret_cast<const float4*>(&sB[(k0 + p + 3) * kWideBP + xc * 4]);
+        acc.x = fmaf(d.x, b0.x, acc.x); acc.y = fmaf(d.x, b0.y, acc.y); acc.z = fmaf(d.x, b0.z, acc.z); acc.w = fmaf(d.x, b0.w, acc.w);
+        acc.x = fmaf(d.y, b1.x, acc.x); acc.y = fmaf(d.y, b1.y, acc.y); acc.z = fmaf(d.y, b1.z, acc.z); acc.w = fmaf(d.y, b1.w, acc.w);
+        acc.x = fmaf(d.z, b2.x, acc.x); acc.y = fmaf(d.z, b2.y, acc.y); acc.z = fmaf(d.z, b2.z, acc.z); acc.w = fmaf(d.z, b2.w, acc.w);
+        acc.x = fmaf(d.w, b3.x, acc.x); acc.y = fmaf(d.w, b3.y, acc.y); acc.z = fmaf(d.w, b3.z, acc.z); acc.w = fmaf(d.w, b3.w, acc.w);
+      }
+      __syncthreads();  // every read of the block's rows done
+      *reinterpret_cast<float4*>(&sB[(k0 + xr) * kWideBP + xc * 4]) = acc;
+      __syncthreads();
+    }
+    if (Rp <= 0) continue;
+    // B rows below -= L_below,k x_k over the padded height (the rows past w
+    // have zero L rows and stay zero)
+    const float* Ls = sL + (size_t)(k & 1) * kWideLBUF;
+    switch ((Rp + 63) >> 6) {
+      case 8: wide_update8<8>(sB, Ls, r0, Rp, k0, tx, ty); break;
+      case 7: wide_update8<7>(sB, Ls, r0, Rp, k0, tx, ty); break;
+      case 6: wide_update8<6>(sB, Ls, r0, Rp, k0, tx, ty); break;
+      case 5: wide_update8<5>(sB, Ls, r0, Rp, k0, tx, ty); break;
+      case 4: wide_update8<4>(sB, Ls, r0, Rp, k0, tx, ty); break;
+      case 3: wide_update8<3>(sB, Ls, r0, Rp, k0, tx, ty); break;
+      case 2: wide_update8<2>(sB, Ls, r0, Rp, k0, tx, ty); break;
+      default: wide_update8<1>(sB, Ls, r0, Rp, k0, tx, ty); break;
+    }
+  }
+  __syncthreads();
+  for (int idx = tid; idx < w * 32; idx += kWideNT) {
+    const int r = idx >> 5, c = idx & 31;
+    if (c < nc) B[(int64_t)r * ldb + c0 + c] = sB[r * kWideBP + c];
+  }
+}
+
 constexpr int TB = 64;  // rows per TRSV block
 
 // Inverse of the diagonal tile, computed by each pipeline CTA before it
@@ -592,6 +799,33 @@ int launch_trsm_llu_block(const float* L, int64_t ldl, float* B, int64_t ldb, in
   return LU_OK;
 }
 
+// dinv: device scratch of 16 x 1024 floats (the diagonal-block inverses)
+int launch_trsm_wide(const float* L, int64_t ldl, float* B, int64_t ldb, int w, int ncols, float* dinv,
+                     cudaStream_t s) {
+  if (w <= 0 || ncols <= 0) return LU_OK;
+  if (w > kWideMaxW || !dinv) return LU_ERR_ARG;
+  static PerDeviceOnce once;
+  LUB_TRY(once_per_device(once, [] {
+    LUB_CUDA(cudaFuncSetAttribute(trsm_wide_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kWideSmem));
+    LUB_CUDA(cudaFuncSetAttribute(trsm_wide_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kWideSmem));
+    return LU_OK;
+  }));
+  const int nkb = ceil_div(w, 32);
+  tri_inv32_kernel<<<nkb, 32, 0, s>>>(L, ldl, w, dinv);
+  LUB_LAUNCH_CHECK();
+  const bool vec = ((reinterpret_cast<uintptr_t>(L) | reinterpret_cast<uintptr_t>(B)) & 15) == 0 &&
+                   (ldl & 3) == 0 && (ldb & 3) == 0;
+  const unsigned grid = (unsigned)ceil_div(ncols, kWideCB);
+  if (vec)
+    trsm_wide_kernel<true><<<grid, kWideNT, kWideSmem, s>>>(L, ldl, dinv, B, ldb, w, ncols);
+  else
+    trsm_wide_kernel<false><<<grid, kWideNT, kWideSmem, s>>>(L, ldl, dinv, B, ldb, w, ncols);
+  LUB_LAUNCH_CHECK();
+  return LU_OK;
+}
+
 template <typename TS, typename T>
 int launch_trsv_mixed(const TS* LU, int64_t lda, int n, T* x, int upper, int* flags, unsigned* ticket, DevStatus* st,
                       long long spin, cudaStream_t s) {
@@ -677,4 +911,16 @@ extern "C" __attribute__((visibility("default"))) int lub_test_wait_timeout(long
 extern "C" __attribute__((visibility("default"))) int lub_test_trsm_block(const float* L, int64_t ldl, float* B,
                                                                         int64_t ldb, int w, int ncols, void* stream) {
   return lub::launch_trsm_llu_block(L, ldl, B, ldb, w, ncols, (cudaStream_t)stream);
+}
+
+// Test hook (not part of include/lu_b200.h): the wide block forward
+// substitution with its own diagonal-inverse scratch.
+extern "C" __attribute__((visibility("default"))) int lub_test_trsm_wide(const float* L, int64_t ldl, float* B,
+                                                                       int64_t ldb, int w, int ncols, void* stream) {
+  float* dinv = nullptr;
+  if (cudaMalloc(&dinv, sizeof(float) * 16 * 1024) != cudaSuccess) return LU_ERR_CUDA;
+  int rc = lub::launch_trsm_wide(L, ldl, B, ldb, w, ncols, dinv, (cudaStream_t)stream);
+  cudaStreamSynchronize((cudaStream_t)stream);
+  cudaFree(dinv);
+  return rc;
 }
