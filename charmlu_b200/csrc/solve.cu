@@ -427,10 +427,14 @@ __global__ void __launch_bounds__(256) trsv_kernel(const TS* LU, int64_t lda, in
   for (int i = 0; i < 8; i++) acc[i] = T(0);
   const int nvisit = UPPER ? (nblk - 1 - bi) : bi;
   bool ok = true;
-  // this warp's 8 rows of tile q (registers): the next tile's loads are in
-  // flight while the warp waits for the current block
+  // a ring of D tiles in registers (this warp's 8 rows of tiles q ..
+  // q + D - 1): D - 1 tiles' loads are in flight while tile q is applied,
+  // and a tile's slice of x is loaded with it when its block is already
+  // known final (otherwise after the wait)
+  constexpr int D = sizeof(TS) == 4 ? 4 : 2;
+  auto col0 = [&](int q) { return (UPPER ? nblk - 1 - q : q) * TB; };
   auto load_tile = [&](int q, TS (&dst)[8][2]) {
-    const int c0 = (UPPER ? nblk - 1 - q : q) * TB;
+    const int c0 = col0(q);
 #pragma unroll
     for (int i = 0; i < 8; i++) {
       const int r = r0 + warp * 8 + i;
@@ -441,30 +445,44 @@ __global__ void __launch_bounds__(256) trsv_kernel(const TS* LU, int64_t lda, in
       }
     }
   };
-  TS lv[8][2], lvn[8][2];
-  if (nvisit > 0) load_tile(0, lv);
+  auto load_x = [&](int q, T (&xd)[2]) {
+    const int c = col0(q) + lane * 2;
+    xd[0] = c < n ? __ldcg(&x[c]) : T(0);
+    xd[1] = c + 1 < n ? __ldcg(&x[c + 1]) : T(0);
+  };
+  TS ring[D][8][2];
+  T xr[D][2];
+  bool xok[D];
   int seen = 0;
-  for (int q = 0; q < nvisit && ok; q++) {
-    const int cb = UPPER ? nblk - 1 - q : q;
-    const int c0 = cb * TB;
-    if (q + 1 < nvisit) load_tile(q + 1, lvn);
-    if (q + 1 > seen) {  // block q (in ticket order) not known to be final yet
-      int v = 0;
-      if (lane == 0) ok = wait_progress(&flags[0], q + 1, &v, st, spin, 301);
-      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-      seen = __shfl_sync(0xffffffffu, v, 0);
-      __syncwarp();  // lane 0's acquire orders the other lanes' reads of x
-      if (!ok) break;
+#pragma unroll
+  for (int d = 0; d < D - 1; d++) {
+    if (d < nvisit) {
+      load_tile(d, ring[d]);
+      xok[d] = false;
     }
-    const int c = c0 + lane * 2;
-    const T x0 = c < n ? __ldcg(&x[c]) : T(0);
-    const T x1 = c + 1 < n ? __ldcg(&x[c + 1]) : T(0);
+  }
+  for (int q0 = 0; q0 < nvisit && ok; q0 += D) {
 #pragma unroll
-    for (int i = 0; i < 8; i++) acc[i] = fma((T)lv[i][1], x1, fma((T)lv[i][0], x0, acc[i]));
+    for (int d = 0; d < D; d++) {
+      const int q = q0 + d;
+      if (q >= nvisit || !ok) break;
+      const int qn = q + D - 1, dn = (d + D - 1) % D;
+      if (qn < nvisit) {
+        load_tile(qn, ring[dn]);
+        xok[dn] = qn < seen;
+        if (xok[dn]) load_x(qn, xr[dn]);
+      }
+      if (q + 1 > seen) {  // block q (in ticket order) not known to be final yet
+        int v = 0;
+        if (lane == 0) ok = wait_progress(&flags[0], q + 1, &v, st, spin, 301);
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+        seen = __shfl_sync(0xffffffffu, v, 0);
+        __syncwarp();  // lane 0's acquire orders the other lanes' reads of x
+        if (!ok) break;
+      }
+      if (!xok[d]) load_x(q, xr[d]);
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      lv[i][0] = lvn[i][0];
-      lv[i][1] = lvn[i][1];
+      for (int i = 0; i < 8; i++) acc[i] = fma((T)ring[d][i][1], xr[d][1], fma((T)ring[d][i][0], xr[d][0], acc[i]));
     }
   }
 #pragma unroll
