@@ -52,7 +52,7 @@ struct lu_handle_s {
   cudaEvent_t evR = nullptr;  // split look-ahead: the rest's operands are built
   // mixed look-ahead: interchanges, U solve and operands of the next panel's
   // columns first, the rest after the panel has started (LU_B200_LA_SPLIT)
-  int la_split = 0;
+  int la_split = 1;  // mixed look-ahead: the next panel's columns first, then the rest
   // leaf tuning: recursion leaf width and CTA cap, without / with look-ahead
   int leaf_w64 = 32, leaf_w32 = 64, leaf_ctas = 148;
   int leaf_w64_la = 16, leaf_w32_la = 32, leaf_ctas_la = 48;
