@@ -96,3 +96,26 @@ def test_cli_process_entry_point(cuda_dev):
     assert r.returncode == 0, r.stderr
     m = RESIDUAL.search(r.stdout)
     assert m is not None and float(m.group(1)) < 16, r.stdout
+
+
+def test_cli_two_ranks_under_torchrun(cuda_dev):
+    """The multi-process FP64 path (`_main_ranks`): two ranks under torchrun,
+    one GPU each, print the reference's result block with residual < 16.
+    Needs two GPUs; skipped otherwise."""
+    import socket
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    env = dict(os.environ, NCCL_NVLS_ENABLE="0")
+    cmd = ["timeout", "-k", "30", "600", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           "--nproc-per-node=2", "--master-addr", "127.0.0.1", "--master-port", str(port), "-m", "charmlu_b200",
+           "2048", "128", "100"]
+    out = subprocess.run(cmd, capture_output=True, text=True, env=env,
+                         cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    assert out.returncode == 0, out.stderr[-2000:]
+    m = RESIDUAL.search(out.stdout)
+    assert m is not None, out.stdout[-2000:]
+    assert float(m.group(1)) < 16
