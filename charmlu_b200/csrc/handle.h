@@ -72,7 +72,8 @@ struct lu_handle_s {
   // mixed path: the panels' inner TRSMs (w <= 256) as one blocked launch
   // instead of the recursion (LU_B200_TRSM_BLOCK=0 restores the recursion)
   int trsm_block = 1;
-  int trsm_wide = 1;  // mixed U block-row solves (w <= 512, > 512 columns) in one launch with inverted diagonal blocks
+  int trsm_wide = 1;  // mixed U block-row solves (w <= 512, > trsm_wide_min columns) in one launch with inverted diagonal blocks
+  int trsm_wide_min = 512;
   lub::TsluScratch tslu_scr{};
   // FP16x3 mixed path: the recursive FP32 panel's GEMM halves of width >= 128
   // on the tcgen05 kernel, with their own split-operand buffers (the panel

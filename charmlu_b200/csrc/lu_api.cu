@@ -346,6 +346,7 @@ int lu_create(const lu_config* cfg, lu_handle* out) {
   if (const char* e = getenv("LU_B200_TSLU")) h->tslu = atoi(e) != 0;
   if (const char* e = getenv("LU_B200_TRSM_BLOCK")) h->trsm_block = std::max(0, std::min(2, atoi(e)));
   if (const char* e = getenv("LU_B200_TRSM_WIDE")) h->trsm_wide = atoi(e) != 0;
+  if (const char* e = getenv("LU_B200_TRSM_WIDE_MIN")) h->trsm_wide_min = std::max(0, atoi(e));
   if (const char* e = getenv("LU_B200_STAGE_BYTES")) h->stage_bytes = std::max<size_t>(1 << 16, strtoull(e, nullptr, 10));
   if (const char* e = getenv("LU_B200_RESIDENT_BYTES")) h->resident_cap = strtoull(e, nullptr, 10);
   if (s == LU_OK) s = h->alloc(&h->perm, n);

@@ -131,7 +131,7 @@ int trsm32(Ctx32& c, int r0, int w, int rb, int cb, int ncols) {
   }
   // a step's U block row (every trailing column): one launch, 32 x 32
   // diagonal blocks inverted first
-  if (w > 32 && w <= 512 && ncols > 512 && c.h->trsm_wide) {
+  if (w > 32 && w <= 512 && ncols > c.h->trsm_wide_min && c.h->trsm_wide) {
     Prof pf(c.h, c.s, LU_PH_TRSM, (double)w * w * ncols);
     return launch_trsm_wide(c.A + (int64_t)r0 * c.ld + r0, c.ld, c.A + (int64_t)rb * c.ld + cb, c.ld, w, ncols,
                             c.h->dinv32, c.s);
