@@ -963,14 +963,16 @@ def main():
                 "executed_note": f"{prods} tensor-core product(s) per element ({args.precision})",
                 "peak_source": peak_src}
         if args.lookahead and gemm_tf:
-            # beside the look-ahead panel the rest of each update runs on the
-            # SMs the panel's reserve leaves it: its fraction of those SMs' peak
+            # beside the look-ahead panel the update's main launch holds the
+            # SMs the panel's reserve leaves it; a helper launch takes the
+            # reserved SMs once the panel is done, so the phase runs on
+            # between these and all SMs
             try:
                 sms = torch.cuda.get_device_properties(dev).multi_processor_count
                 held = sms - int(os.environ.get("LU_B200_GEMM_RESERVE", "48"))
                 if 0 < held < sms:
-                    roof["sms_held"] = held
-                    roof["frac_executed_of_sms_held"] = gemm_tf / (peak_v * held / sms)
+                    roof["sms_beside_panel"] = held
+                    roof["sms_total"] = sms
             except Exception:
                 pass
         tpath = os.path.join(ROOT, "profiles",
