@@ -341,7 +341,10 @@ int factor_mixed_split_step(lu_handle h, Ctx32& c, Ctx32& cp, const CUtensorMap&
 
 // LU of h->A32 in place: FP32 panels/TRSM, low-precision tcgen05 trailing
 // updates; with look-ahead, panel k+1 overlaps the rest of update k.
-int factor_mixed(lu_handle h, cudaStream_t s) {
+// rest_src (look-ahead only): h->A32 holds only the first panel's columns;
+// the FP64 source of the other columns (leading dimension rest_lda) is
+// converted on the main stream while the first panel is factored.
+int factor_mixed(lu_handle h, cudaStream_t s, const double* rest_src, int64_t rest_lda) {
   const int n = (int)h->cfg.n, B = h->cfg.block_size;
   const bool bf16 = h->cfg.precision == LU_PREC_BF16;
   const bool la = h->cfg.lookahead != 0;
@@ -381,6 +384,10 @@ int factor_mixed(lu_handle h, cudaStream_t s) {
   LUB_TRY(panel32(cp, 0, std::min(B, n), 0, std::min(B, n)));
   if (h->capturing) LUB_TRY(mark_branch_priority(h, h->sP, mark));
   LUB_CUDA(cudaEventRecord(h->evP, h->sP));
+  if (rest_src && B < n) {
+    Prof pf(h, s, LU_PH_OTHER);
+    LUB_TRY(launch_f64_to_f32(rest_src + B, rest_lda, h->A32 + B, h->ld32, n, n - B, s));
+  }
   const bool split = h->la_split && h->pairs && !bf16;
   for (int k0 = 0; k0 < n; k0 += B) {
     const int kw = std::min(B, n - k0), k1 = k0 + kw, rest = n - k1;
@@ -681,11 +688,14 @@ int mixed_factor(lu_handle h, const double* A, int64_t lda, cudaStream_t s) {
   LUB_TRY(ensure_mixed(h));
   LUB_CUDA(cudaMemsetAsync(h->st, 0, sizeof(DevStatus), s));
   return run_graph(h, 1, A, h->A32, nullptr, lda, s, [&](cudaStream_t ss) {
+    // with look-ahead the first panel starts once its own columns are in
+    // FP32; the other columns are converted beside it
+    const int b0 = h->cfg.lookahead ? std::min<int>((int)h->cfg.block_size, n) : n;
     {
       Prof pf(h, ss, LU_PH_OTHER);
-      LUB_TRY(launch_f64_to_f32(A, lda, h->A32, h->ld32, n, n, ss));
+      LUB_TRY(launch_f64_to_f32(A, lda, h->A32, h->ld32, n, b0, ss));
     }
-    return factor_mixed(h, ss);
+    return factor_mixed(h, ss, b0 < n ? A : nullptr, lda);
   });
 }
 
@@ -704,7 +714,7 @@ int mixed_factor_host(lu_handle h, const ASrc& a, cudaStream_t s) {
       return launch_f64_to_f32(rows_dev, a.lda, h->A32 + (int64_t)r0 * h->ld32, h->ld32, rows, n, s);
     }));
   }
-  return factor_mixed(h, s);
+  return factor_mixed(h, s, nullptr, 0);
 }
 
 int refine_solve(lu_handle h, const ASrc& A, const double* b, double* x, lu_refine_info* info, cudaStream_t s) {
