@@ -3,10 +3,12 @@
 // its panel and triangular solves in FP32 (only the trailing update drops to
 // BF16 tensor cores), so these run on the FP32 SIMT pipe.
 //
-// Tiling: CTA 128 x 128, K-tile 16, 256 threads with an 8 x 8 register
-// block each (outer products from shared memory); the A tile is stored
-// k-major in shared memory so both operands are read as float4.  Tiles are
-// double-buffered through registers; edges are zero-filled on load.
+// Tiling: CTA 128 x 128, K-tile 16, 256 threads with a 16 x 4 register
+// block each (outer products from shared memory): warp w owns rows
+// 16 w .. 16 w + 15 and lane l columns 4 l .. 4 l + 3, so per k the A values
+// are warp-wide broadcasts (four float4 loads, one wavefront each) and the B
+// values one float4 per lane.  The A tile is stored k-major in shared memory.
+// Tiles are double-buffered through registers; edges are zero-filled on load.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -22,7 +24,7 @@ gemm_f32_sub_kernel(const float* __restrict__ A, int64_t lda, const float* __res
   __shared__ __align__(16) float Bs[2][BK][BN + 4];
   const int tid = threadIdx.x;
   const int tm = blockIdx.y * BM, tn = blockIdx.x * BN;
-  const int tx = tid & 15, ty = tid >> 4;  // 16 x 16 threads, 8 x 8 each
+  const int tx = tid & 31, ty = tid >> 5;  // 32 column groups x 8 row groups, 16 x 4 each
 
   // loader mapping: A tile 128 x 16 -> each thread 8 elements (rows ar, ar+64; k ak..ak+3)
   const int ar = tid >> 2, ak = (tid & 3) * 4;
@@ -56,11 +58,11 @@ gemm_f32_sub_kernel(const float* __restrict__ A, int64_t lda, const float* __res
     }
   };
 
-  float acc[8][8];
+  float acc[16][4];
 #pragma unroll
-  for (int i = 0; i < 8; i++)
+  for (int i = 0; i < 16; i++)
 #pragma unroll
-    for (int j = 0; j < 8; j++) acc[i][j] = 0.f;
+    for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
 
   const int KT = (K + BK - 1) / BK;
   load(0);
@@ -71,30 +73,32 @@ gemm_f32_sub_kernel(const float* __restrict__ A, int64_t lda, const float* __res
     if (kt + 1 < KT) load((kt + 1) * BK);
 #pragma unroll
     for (int k = 0; k < BK; k++) {
-      const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][k][ty * 4]);
-      const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][k][64 + ty * 4]);
-      const float4 b0 = *reinterpret_cast<const float4*>(&Bs[buf][k][tx * 4]);
-      const float4 b1 = *reinterpret_cast<const float4*>(&Bs[buf][k][64 + tx * 4]);
-      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+      float av[16];
 #pragma unroll
-      for (int i = 0; i < 8; i++)
+      for (int q = 0; q < 4; q++) {
+        const float4 a = *reinterpret_cast<const float4*>(&As[buf][k][ty * 16 + q * 4]);
+        av[4 * q] = a.x; av[4 * q + 1] = a.y; av[4 * q + 2] = a.z; av[4 * q + 3] = a.w;
+      }
+      const float4 b = *reinterpret_cast<const float4*>(&Bs[buf][k][tx * 4]);
+      const float bv[4] = {b.x, b.y, b.z, b.w};
 #pragma unroll
-        for (int j = 0; j < 8; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+      for (int i = 0; i < 16; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
     }
     if (kt + 1 < KT) {
       store(buf ^ 1);
       __syncthreads();
     }
   }
-  // C -= acc (rows ty*4 + {0..3}, 64 + ty*4 + {0..3}; cols tx*4.., 64 + tx*4..)
+  // C -= acc (rows ty*16 + i, cols tx*4 + j: a warp's row is 128 contiguous floats)
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
-    const int r = tm + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+  for (int i = 0; i < 16; i++) {
+    const int r = tm + ty * 16 + i;
     if (r >= M) continue;
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const int c = tn + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+    for (int j = 0; j < 4; j++) {
+      const int c = tn + tx * 4 + j;
       if (c < N) C[(int64_t)r * ldc + c] -= acc[i][j];
     }
   }
