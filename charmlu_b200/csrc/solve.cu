@@ -49,26 +49,30 @@ __global__ void __launch_bounds__(128) trsm_llu_leaf_kernel(const T* L, int64_t 
 }
 
 // B (w x ncols) <- L^{-1} B, L unit lower w x w (w <= kTrsmBlockMaxW), FP32,
-// in one launch: each CTA keeps a 32-column slice of B in shared memory and
+// in one launch: each CTA keeps a slice of 4-32 columns of B in shared memory and
 // walks down L in 32-row blocks, solving the block's diagonal part (one
 // thread per column, in registers) and then updating the rows below it with
 // the block's columns of L.  This replaces the recursion's chain of small
 // launches (for w = 256: 8 leaf solves and 7 GEMMs) inside the mixed path's
 // panels.
 constexpr int kTrsmBlockMaxW = 256;
-constexpr int kTrsmCB = 32;   // columns of B per CTA
 constexpr int kTrsmNT = 256;
 
+// CB columns of B per CTA (4 .. 32): narrow slices spread a small solve over
+// more SMs; each column's arithmetic is the same for every CB.
+template <int CB>
 __global__ void __launch_bounds__(kTrsmNT) trsm_llu_block_kernel(const float* __restrict__ L, int64_t ldl,
                                                                  float* __restrict__ B, int64_t ldb, int w,
                                                                  int ncols) {
-  __shared__ float sB[kTrsmBlockMaxW][kTrsmCB + 1];
+  constexpr int TXN = CB / 4;          // groups of 4 columns
+  constexpr int RS = kTrsmNT / TXN;    // rows updated in parallel
+  __shared__ float sB[kTrsmBlockMaxW][CB + 1];
   __shared__ float sL[32][33];
   const int tid = threadIdx.x;
-  const int c0 = blockIdx.x * kTrsmCB;
-  const int nc = min(kTrsmCB, ncols - c0);
-  for (int idx = tid; idx < w * kTrsmCB; idx += kTrsmNT) {
-    const int r = idx / kTrsmCB, c = idx - r * kTrsmCB;
+  const int c0 = blockIdx.x * CB;
+  const int nc = min(CB, ncols - c0);
+  for (int idx = tid; idx < w * CB; idx += kTrsmNT) {
+    const int r = idx / CB, c = idx - r * CB;
     sB[r][c] = c < nc ? B[(int64_t)r * ldb + c0 + c] : 0.f;
   }
   for (int k0 = 0; k0 < w; k0 += 32) {
@@ -79,7 +83,7 @@ __global__ void __launch_bounds__(kTrsmNT) trsm_llu_block_kernel(const float* __
     }
     __syncthreads();
     // the diagonal block: forward substitution down each column
-    if (tid < kTrsmCB) {
+    if (tid < CB) {
       float x[32];
 #pragma unroll
       for (int i = 0; i < 32; i++) x[i] = i < kb ? sB[k0 + i][tid] : 0.f;
@@ -94,8 +98,8 @@ __global__ void __launch_bounds__(kTrsmNT) trsm_llu_block_kernel(const float* __
     }
     __syncthreads();
     // the rows below: B[r, :] -= L[r, k0:k0+kb] B[k0:k0+kb, :], 4 columns per thread
-    const int tx = tid & 7, ty = tid >> 3;
-    for (int r = k0 + kb + ty; r < w; r += kTrsmNT / 8) {
+    const int tx = tid % TXN, ty = tid / TXN;
+    for (int r = k0 + kb + ty; r < w; r += RS) {
       const float* lr = L + (int64_t)r * ldl + k0;
       float a0 = sB[r][4 * tx], a1 = sB[r][4 * tx + 1], a2 = sB[r][4 * tx + 2], a3 = sB[r][4 * tx + 3];
       for (int p = 0; p < kb; p++) {
@@ -112,8 +116,8 @@ __global__ void __launch_bounds__(kTrsmNT) trsm_llu_block_kernel(const float* __
     }
     __syncthreads();
   }
-  for (int idx = tid; idx < w * kTrsmCB; idx += kTrsmNT) {
-    const int r = idx / kTrsmCB, c = idx - r * kTrsmCB;
+  for (int idx = tid; idx < w * CB; idx += kTrsmNT) {
+    const int r = idx / CB, c = idx - r * CB;
     if (c < nc) B[(int64_t)r * ldb + c0 + c] = sB[r][c];
   }
 }
@@ -812,7 +816,15 @@ int launch_trsm_llu_leaf(const T* L, int64_t ldl, T* B, int64_t ldb, int m, int 
 int launch_trsm_llu_block(const float* L, int64_t ldl, float* B, int64_t ldb, int w, int ncols, cudaStream_t s) {
   if (w <= 1 || ncols <= 0) return LU_OK;
   if (w > kTrsmBlockMaxW) return LU_ERR_ARG;
-  trsm_llu_block_kernel<<<ceil_div(ncols, kTrsmCB), kTrsmNT, 0, s>>>(L, ldl, B, ldb, w, ncols);
+  // slices narrow enough for at least ~32 CTAs
+  if (ncols >= 1024)
+    trsm_llu_block_kernel<32><<<ceil_div(ncols, 32), kTrsmNT, 0, s>>>(L, ldl, B, ldb, w, ncols);
+  else if (ncols >= 512)
+    trsm_llu_block_kernel<16><<<ceil_div(ncols, 16), kTrsmNT, 0, s>>>(L, ldl, B, ldb, w, ncols);
+  else if (ncols >= 256)
+    trsm_llu_block_kernel<8><<<ceil_div(ncols, 8), kTrsmNT, 0, s>>>(L, ldl, B, ldb, w, ncols);
+  else
+    trsm_llu_block_kernel<4><<<ceil_div(ncols, 4), kTrsmNT, 0, s>>>(L, ldl, B, ldb, w, ncols);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }
