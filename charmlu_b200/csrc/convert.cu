@@ -79,26 +79,54 @@ __global__ void split_transpose_kernel(const float* __restrict__ src, int64_t ld
   }
 }
 
-// amax[0] = max |L| over rows x K, amax[1] = max |U| over K x N (bit patterns)
+// max |P| over a rows x cols row-major block: warps take segments of up to
+// 2048 columns of one row (one division per segment), lanes read float4 when
+// the block allows 16-byte loads
+__device__ __forceinline__ float absmax_block(const float* __restrict__ P, int64_t ld, int rows, int cols, int gw,
+                                             int nw, int lane) {
+  constexpr int SEG = 2048;
+  float m = 0.f;
+  if (rows <= 0 || cols <= 0) return m;
+  const int nseg = (cols + SEG - 1) / SEG;
+  const int64_t units = (int64_t)rows * nseg;
+  const bool vec = ((reinterpret_cast<uintptr_t>(P) & 15) == 0) && ((ld & 3) == 0) && ((cols & 3) == 0);
+  for (int64_t u = gw; u < units; u += nw) {
+    const int64_t r = u / nseg;
+    const int c0 = (int)(u - r * nseg) * SEG, c1 = min(cols, c0 + SEG);
+    const float* row = P + r * ld;
+    if (vec) {
+#pragma unroll 4
+      for (int c = c0 + 4 * lane; c < c1; c += 128) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(row + c));
+        m = fmaxf(m, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+      }
+    } else {
+#pragma unroll 4
+      for (int c = c0 + lane; c < c1; c += 32) m = fmaxf(m, fabsf(row[c]));
+    }
+  }
+  return m;
+}
+
+// amax[0] = max |L| (rows x K), or *lmax_from when given; amax[1] = max |U|
+// (K x N); float bit patterns (non-negative floats order as unsigned)
 __global__ void panel_absmax_kernel(const float* __restrict__ L, int64_t ldl, int rows, int K,
-                                    const float* __restrict__ U, int64_t ldu, int N, unsigned* amax) {
-  float mL = 0.f, mU = 0.f;
-  const int64_t totL = (int64_t)rows * K, totU = (int64_t)K * N;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < totL; i += stride) {
-    const int64_t r = i / K, k = i - r * K;
-    mL = fmaxf(mL, fabsf(L[r * ldl + k]));
-  }
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < totU; i += stride) {
-    const int64_t k = i / N, c = i - k * N;
-    mU = fmaxf(mU, fabsf(U[k * ldu + c]));
-  }
+                                    const float* __restrict__ U, int64_t ldu, int N, unsigned* amax,
+                                    const unsigned* lmax_from) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+  float mL = lmax_from ? 0.f : absmax_block(L, ldl, rows, K, gw, nw, lane);
+  float mU = absmax_block(U, ldu, K, N, gw, nw, lane);
   for (int o = 16; o > 0; o >>= 1) {
     mL = fmaxf(mL, __shfl_xor_sync(0xffffffffu, mL, o));
     mU = fmaxf(mU, __shfl_xor_sync(0xffffffffu, mU, o));
   }
-  if ((threadIdx.x & 31) == 0) {
-    atomicMax(&amax[0], __float_as_uint(mL));
+  if (lane == 0) {
+    if (lmax_from) {
+      if (gw == 0) atomicMax(&amax[0], *lmax_from);
+    } else {
+      atomicMax(&amax[0], __float_as_uint(mL));
+    }
     atomicMax(&amax[1], __float_as_uint(mU));
   }
 }
@@ -260,11 +288,11 @@ template int launch_split_transpose<__half>(const float*, int64_t, __half*, int6
                                             const unsigned*, int, cudaStream_t, int);
 
 int launch_panel_absmax(const float* L, int64_t ldl, int rows, int K, const float* U, int64_t ldu, int N,
-                        unsigned* amax, cudaStream_t s) {
+                        unsigned* amax, cudaStream_t s, const unsigned* lmax_from) {
   LUB_CUDA(cudaMemsetAsync(amax, 0, 2 * sizeof(unsigned), s));
-  const int64_t tot = std::max((int64_t)rows * K, (int64_t)K * N);
-  const int blocks = (int)std::min<int64_t>(std::max<int64_t>(1, tot / 2048), 4 * kNumSMsB200);
-  panel_absmax_kernel<<<blocks, 256, 0, s>>>(L, ldl, rows, K, U, ldu, N, amax);
+  const int64_t tot = std::max(lmax_from ? 0 : (int64_t)rows * K, (int64_t)K * N);
+  const int blocks = (int)std::min<int64_t>(std::max<int64_t>(1, tot / 4096), 4 * kNumSMsB200);
+  panel_absmax_kernel<<<blocks, 256, 0, s>>>(L, ldl, rows, K, U, ldu, N, amax, lmax_from);
   LUB_LAUNCH_CHECK();
   return LU_OK;
 }

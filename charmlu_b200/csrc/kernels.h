@@ -175,9 +175,10 @@ int launch_gemm_lowp_persistent(const CUtensorMap& mapA, const CUtensorMap& mapB
                                 int a_row0, int b_row0, int c_row0, int c_col0, int M, int N, int K, bool bf16,
                                 const unsigned* amax, DevStatus* st, long long spin, int max_ctas, cudaStream_t s,
                                 int kpart = 0, unsigned* tile_ctr = nullptr, bool cta_pair = false);
-// |max| of the L21 (rows x K) and U12 (K x N) FP32 panels into amax[0], amax[1]
+// |max| of the L21 (rows x K) and U12 (K x N) FP32 panels into amax[0], amax[1];
+// lmax_from: take amax[0] from there instead of reading L (the same L21)
 int launch_panel_absmax(const float* L, int64_t ldl, int rows, int K, const float* U, int64_t ldu, int N,
-                        unsigned* amax, cudaStream_t s);
+                        unsigned* amax, cudaStream_t s, const unsigned* lmax_from = nullptr);
 // low-precision operand panels: nparts K-wide copies, part p is the hi
 // (bit p of lo_mask clear) or lo (set) component of src * scale, scale the
 // power of two of amax[which] (or 1 when amax is null); OUT bf16 or fp16

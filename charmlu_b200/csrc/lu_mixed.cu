@@ -255,7 +255,8 @@ int build_operands_part(lu_handle h, const Ctx32& c, int k0, int kw, int k1, int
   *kpart = kps;
   {
     Prof pf(h, s, LU_PH_OTHER);
-    LUB_TRY(launch_panel_absmax(L21, c.ld, rest, kw, U12, c.ld, ncols, amax, s));
+    // a later part of the same step has L21's maximum already (amax pair 0)
+    LUB_TRY(launch_panel_absmax(L21, c.ld, rest, kw, U12, c.ld, ncols, amax, s, with_l ? nullptr : h->amax));
     if (with_l)
       LUB_TRY(launch_split_rows<__half>(L21, c.ld, reinterpret_cast<__half*>(h->Lb), h->ldk, rest, kw, 2, 0x2u, amax,
                                         0, s, kps));
