@@ -106,11 +106,15 @@ inline int split_w32(int w) {
   return std::max(w1, 4);
 }
 
-int pivots_apply_f32(Ctx32& c, int k0, int cnt, int c_begin, int c_end, int skip_b, int skip_e, int32_t* perm) {
+// composed: the context's pivot list already holds this batch (cnt <= 512),
+// composed by an earlier call on the same stream
+int pivots_apply_f32(Ctx32& c, int k0, int cnt, int c_begin, int c_end, int skip_b, int skip_e, int32_t* perm,
+                     bool composed = false) {
   Prof pf(c.h, c.s, LU_PH_LASWP);
+  if (composed && cnt > 512) return LU_ERR_ARG;
   for (int off = 0; off < cnt; off += 512) {
     const int sub = std::min(512, cnt - off);
-    LUB_TRY(launch_pivot_compose(c.ipiv, k0 + off, sub, c.pl, c.s));
+    if (!composed) LUB_TRY(launch_pivot_compose(c.ipiv, k0 + off, sub, c.pl, c.s));
     LUB_TRY(launch_pivot_apply<float>(c.A, c.ld, c_begin, c_end, skip_b, skip_e, c.pl, 2 * sub, nullptr, perm, c.s));
   }
   return LU_OK;
@@ -319,7 +323,7 @@ int factor_mixed_split_step(lu_handle h, Ctx32& c, Ctx32& cp, const CUtensorMap&
   if (h->capturing) LUB_TRY(mark_branch_priority(h, h->sP, mark));
   // every other column: the left L columns, and the trailing ones past the
   // next panel (the panel's own columns are being factored beside this)
-  LUB_TRY(pivots_apply_f32(c, k0, kw, 0, n, k0, k1 + nw, h->perm));
+  LUB_TRY(pivots_apply_f32(c, k0, kw, 0, n, k0, k1 + nw, h->perm, kw <= 512));
   if (rest == nw) {
     LUB_CUDA(cudaEventRecord(h->evP, h->sP));
     return LU_OK;
