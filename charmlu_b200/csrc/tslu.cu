@@ -206,7 +206,7 @@ __device__ __forceinline__ int warp_find(const int* key, int n, int v) {
 // 2. The tournament's later rounds.  CTA b stacks the candidate sets
 //    [b * group, (b + 1) * group) of the previous round (their rows'
 //    original values) and factors the stack with partial pivoting; the rows
-//    it chooses form set b of this round.  The final round (one CTA, FINAL)
+//    it chooses form set b of this tournament round.  The final round (one CTA, FINAL)
 //    instead turns its choice into ipiv, L11\U11, the row moves and the
 //    moved rows' data.
 template <int W, bool FINAL>

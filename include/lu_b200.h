@@ -270,8 +270,8 @@ LU_API int lu_batched_factor_solve(int32_t count, const int32_t* n, const int64_
 LU_API size_t lu_batched_work_bytes(int32_t count, const int32_t* n_host, int32_t precision);
 /* After an LU_PREC_FP32 lu_batched_factor_solve on dWork (device), once the
  * stream reaches it: hist[s] (host, 12 entries) = systems whose scaled
- * residual was below 16 after s FP64 refinement steps (s = 0 .. 10; the
- * north star's one step is s = 1), hist[11] = systems that did not get
+ * residual was below 16 after s FP64 refinement steps (s = 0 .. 10; a
+ * single refinement step is s = 1), hist[11] = systems that did not get
  * there.  Synchronises.  No reference counterpart. */
 LU_API int lu_batched_refine_histogram(const void* dWork, int32_t* hist, void* stream);
 /* Per-size-bucket kernel parameters chosen by the autotuner: entries of

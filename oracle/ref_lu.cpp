@@ -2,7 +2,7 @@
 //
 // A CPU restatement of charmlu's dense LU hot path (factor with partial
 // pivoting, block forward/backward substitution, scaled-residual check).  It
-// is the checker for the CUDA path in charmlu_b200 and the timed CPU baseline
+// is the parity reference for the CUDA path in charmlu_b200 and the timed CPU baseline
 // ("kind": "port").  Nothing in the product library links or calls it; only
 // tests/, __graft_entry__.smoke() and bench.py (cpu_baseline / --impl
 // reference) load it.

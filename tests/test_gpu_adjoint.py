@@ -1,6 +1,6 @@
 """Adjoint of X = A^{-1} B (no reference counterpart): lu_adjoint and the
 torch.autograd binding against an FP64 reference gradient and central finite
-differences.  Bar (north_star): gradients within 1e-10 relative (normwise)
+differences.  Bar: gradients within 1e-10 relative (normwise)
 of the FP64 reference gradient."""
 import numpy as np
 import pytest

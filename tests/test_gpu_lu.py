@@ -1,6 +1,6 @@
 """GPU parity tests of the FP64 path through the C ABI against the CPU oracle.
 
-Bars (north_star): pivots bit-exact except near-ties (oracle top-2 margin
+Bars: pivots bit-exact except near-ties (oracle top-2 margin
 <= 1e-10, where a different summation order may legitimately flip the
 choice), L and U within 1e-12 relative (max-abs difference over max-abs
 entry), scaled residual < 16.
